@@ -1,0 +1,207 @@
+/*
+ * tvs.h -- C ABI of the B200 total-viewshed engine (libtvs_cuda.so).
+ *
+ * The reference (tombh/total-viewsheds) dispatches each sector to a backend in
+ * Compute::compute_sector (crates/total-viewsheds/src/compute.rs:181-203); its
+ * `ComputeType::Cuda` arm is `unimplemented!()` (compute.rs:197).  These entry
+ * points are what that arm binds through a Rust `extern "C"` block (built by
+ * build.rs): plain pointers and sizes, status codes, no exceptions or aborts
+ * across the boundary.
+ *
+ * Ownership: the caller owns every pointer it passes; the library reads or
+ * writes them before returning.  The library owns its device buffers.
+ * Threading: one context per host thread; calls on one context are serialised
+ * by the caller.  Each context owns one CUDA stream on its device.
+ */
+#ifndef TVS_H
+#define TVS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TVS_ABI_VERSION 1
+
+/* Status codes.  Negative values are errors; tvs_last_error() has the text. */
+enum tvs_status {
+    TVS_OK = 0,
+    TVS_ERR_INVALID_ARGUMENT = -1,
+    /* dem.rs:56-62: line of sight longer than half the DEM width. */
+    TVS_ERR_LOS_TOO_LONG = -2,
+    /* band_of_sight.rs:103-165: the shape window or strip falls outside the
+     * sorted DEM (the reference panics on an index). */
+    TVS_ERR_SHAPE = -3,
+    /* kernel.rs:157-164: a band walks off the DEM (the reference panics on
+     * elevations[dem_id]). */
+    TVS_ERR_PATH_OUT_OF_DEM = -4,
+    /* kernel.rs:302-309: ring records overflow past the end of the sector's
+     * ring buffer (the reference panics on ring_data[index]). */
+    TVS_ERR_RING_OVERFLOW = -5,
+    TVS_ERR_CUDA = -6,
+    TVS_ERR_NO_DEVICE = -7,
+    TVS_ERR_OUT_OF_MEMORY = -8,
+    /* An internal fixed-capacity buffer (shape candidates, ring spill list)
+     * was too small for this input. */
+    TVS_ERR_CAPACITY = -9,
+    /* A device wait gave up after its iteration limit. */
+    TVS_ERR_TIMEOUT = -10
+};
+
+/* Sweep arithmetic.  See kernel.rs:164-233 for the reference expression. */
+enum tvs_precision {
+    /* Bit-exact with the reference f32 kernel: surfaces and ring records. */
+    TVS_PRECISION_EXACT32 = 0,
+    /* FP32 fast path from reciprocal/curvature tables; every comparison within
+     * 8 ulp of the running maximum is re-decided in FP64.  Visibility matches
+     * the all-FP64 sweep; surfaces accumulate in FP64. */
+    TVS_PRECISION_MIXED64 = 1,
+    /* The all-FP64 sweep (angles, running maximum, surfaces in double). */
+    TVS_PRECISION_FP64 = 2
+};
+
+/* Which sweep kernel runs. */
+enum tvs_sweep_kernel {
+    /* The tiled engine: one thread per point of view, both band directions
+     * interleaved, step tables in shared memory. */
+    TVS_SWEEP_ENGINE = 0,
+    /* The plain port of the reference shader: one thread per band, IEEE
+     * divisions, every step of the delta table.  The baseline (EXACT32 only). */
+    TVS_SWEEP_PLAIN = 1
+};
+
+typedef struct tvs_params {
+    uint32_t width;              /* DEM columns (Header.width, input.rs:98)          */
+    uint32_t height;             /* DEM rows; the reference requires height == width */
+    float scale;                 /* metres per cell (--scale, config.rs:51-53)       */
+    uint32_t max_line_of_sight;  /* metres (--max-line-of-sight, config.rs:18-24)    */
+    float rings_per_km;          /* --rings-per-km (config.rs:26-33)                  */
+    float observer_height;       /* metres; compute.rs:41 hard-codes 1.8             */
+    uint32_t precision;          /* enum tvs_precision                               */
+    uint32_t sweep_kernel;       /* enum tvs_sweep_kernel                            */
+    int32_t device;              /* CUDA device ordinal                              */
+    uint32_t tvs_row_begin;      /* computable-grid rows handled by this context:    */
+    uint32_t tvs_row_end;        /* [begin, end); 0,0 = every row                    */
+} tvs_params;
+
+/* Geometry derived as DEM::new (dem.rs:44-72) and Compute::new
+ * (compute.rs:27-56, cfg(test) ring sizing) derive it. */
+typedef struct tvs_geometry {
+    uint32_t width;
+    uint32_t height;
+    uint32_t max_los_as_points;        /* dem.rs:53                               */
+    uint32_t band_size;                /* dem.rs:78                               */
+    uint32_t band_deltas_size;         /* band_of_sight.rs:54-58                  */
+    uint32_t tvs_width;                /* dem.rs:82                               */
+    uint32_t tvs_height;
+    uint32_t reserved_rings_per_band;  /* compute.rs:94-98                        */
+    uint32_t band_samples;             /* band_of_sight.rs:95                     */
+    uint32_t band_steps_filled;        /* entries of the delta table the shape    */
+                                       /* stage fills (band_of_sight.rs:158)      */
+    uint64_t size;                     /* width * height                          */
+    uint64_t computable_points_count;  /* dem.rs:87-115                           */
+    uint64_t total_bands;              /* compute.rs:34                           */
+    uint64_t ring_slots_per_sector;    /* total_bands * reserved_rings_per_band   */
+} tvs_geometry;
+
+typedef struct tvs_sector_stats {
+    uint32_t angle;
+    uint32_t band_steps_filled;
+    uint32_t overflow_bands;     /* bands with more ring ids than reserved slots  */
+    uint32_t max_ring_ids;       /* ring-record high-water mark (ids in one band) */
+    uint64_t spill_entries;      /* ring ids written past their own record        */
+} tvs_sector_stats;
+
+typedef struct tvs_context tvs_context;
+
+/* Called by tvs_run after each sector with that sector's ring records in the
+ * reference layout (kernel.rs:141-145,243), or NULL when the callback asked
+ * for none.  Return non-zero to stop the run. */
+typedef int (*tvs_sector_callback)(void *user, uint32_t angle, const uint32_t *rings,
+                                   uint64_t rings_len, const tvs_sector_stats *stats);
+
+/* ---- lifetime -------------------------------------------------------- */
+
+/* GPU::new (gpu.rs:55-61): validate the geometry, pick the device, allocate,
+ * upload the elevations (row-major, width*height f32). */
+int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_elevations,
+               tvs_context **out);
+void tvs_destroy(tvs_context *ctx);
+/* Last error text of ctx, or of the last failed tvs_create when ctx is NULL. */
+const char *tvs_last_error(const tvs_context *ctx);
+int tvs_abi_version(void);
+
+/* DEM::new + Compute::new geometry, without a context or a GPU. */
+int tvs_compute_geometry(const tvs_params *params, tvs_geometry *out);
+int tvs_get_geometry(const tvs_context *ctx, tvs_geometry *out);
+
+/* Replace the elevations (same size).  main.rs:51-56 converts i16 -> f32. */
+int tvs_set_elevations(tvs_context *ctx, const float *elevations, uint64_t n_elevations);
+
+/* ---- the per-sector stages ------------------------------------------- */
+
+/* Axes::compute (axes.rs:103-130) restricted to what the shape needs:
+ * sector_ordered[first_rank .. first_rank+count) (ids in sector order) and
+ * the f32 sight distances of every point (nullable). */
+int tvs_axes(tvs_context *ctx, uint32_t angle, uint64_t first_rank, uint64_t count,
+             uint32_t *sector_ordered, float *sight_distances);
+
+/* DEM::compile_band_data (band_of_sight.rs:61-174): band_deltas_size entries;
+ * entries past band_steps_filled are 0 as in the reference. */
+int tvs_band_shape(tvs_context *ctx, uint32_t angle, int32_t *band_deltas,
+                   float *band_distances, uint32_t *band_steps_filled);
+
+/* Compute::compute_sector (compute.rs:181-203) for ComputeType::Cuda:
+ * cumulative_surfaces [computable_points_count] is read, advanced by this
+ * sector and written back (kernel.rs:254).  rings (nullable) receives the
+ * sector's ring records in the reference layout; rings_len must be at least
+ * ring_slots_per_sector.  stats is nullable. */
+int tvs_compute_sector(tvs_context *ctx, uint32_t angle, float *cumulative_surfaces,
+                       uint32_t *rings, uint64_t rings_len, tvs_sector_stats *stats);
+
+/* Compute::run (compute.rs:101-115): all 180 sectors.  cumulative_out and
+ * total_out (the heatmap running total, compute.rs:206-214; nullable) have
+ * computable_points_count entries.  callback (nullable) receives each
+ * sector's ring records when want_rings != 0. */
+int tvs_run(tvs_context *ctx, float *cumulative_out, float *total_out, int want_rings,
+            tvs_sector_callback callback, void *user);
+
+/* ---- device-resident form (inputs and outputs stay in HBM) ----------- */
+
+/* Zero the device cumulative and running-total surfaces. */
+int tvs_device_reset(tvs_context *ctx);
+/* Enqueue sectors [first_angle, first_angle+count) on the context's stream
+ * (no host synchronisation, no rings).  Errors surface at tvs_device_finish. */
+int tvs_device_run_sectors(tvs_context *ctx, uint32_t first_angle, uint32_t count);
+/* The two stages of tvs_device_run_sectors, for callers that time them apart:
+ * the shape stage (one CTA per sector) and the sweep (one launch). */
+int tvs_device_shape_sectors(tvs_context *ctx, uint32_t first_angle, uint32_t count);
+int tvs_device_sweep_sectors(tvs_context *ctx, uint32_t first_angle, uint32_t count);
+/* Wait for the stream and report the first error of the sectors enqueued
+ * since the last tvs_device_finish, if any. */
+int tvs_device_finish(tvs_context *ctx);
+/* Copy the device surfaces to the host (either pointer nullable). */
+int tvs_read_surfaces(tvs_context *ctx, float *cumulative_out, float *total_out);
+/* Device pointer of the float32 cumulative surfaces, for zero-copy callers. */
+const float *tvs_device_cumulative(const tvs_context *ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that time on it. */
+void *tvs_stream(const tvs_context *ctx);
+/* Number of kernels the last tvs_device_run_sectors call enqueued. */
+uint64_t tvs_last_launch_count(const tvs_context *ctx);
+
+/* ---- self-checks ------------------------------------------------------ */
+
+/* Compare the sweep's table-driven division with CUDA's IEEE division
+ * (__fdiv_rn) on n pseudo-random (numerator, distance) pairs drawn from
+ * seed; returns the number of bitwise mismatches in *mismatches. */
+int tvs_selftest_division(int32_t device, uint64_t n, uint64_t seed, uint64_t *mismatches);
+
+/* FP32 issue-rate microbenchmark (independent FFMA chains on every SM):
+ * measured FP32 lane-instructions per second, the sweep's roofline peak. */
+int tvs_measure_fp32_issue(int32_t device, double *instructions_per_second);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,98 @@
+"""Properties of the CPU oracle beyond the reference's vectors: the stable radix
+order against a second, independent sort; thread-count invariance; the
+reference's panic cases as error codes; the unfilled delta-table tail."""
+
+import numpy as np
+import pytest
+
+from conftest import f32
+
+
+def radix_key(values32):
+    bits = values32.view(np.uint32)
+    mask = (-(bits >> 31).astype(np.int64)).astype(np.uint32) | np.uint32(0x80000000)
+    return bits ^ mask
+
+
+@pytest.mark.parametrize("width,angle", [(64, 0.0), (64, 33.0), (97, 90.0), (301, 135.0),
+                                         (301, 179.0)])
+def test_order_matches_lexsort(oracle, width, angle):
+    """radsort's stable LSD order == a sort on (f32 key, index)."""
+    d = oracle.calculate_distances(width, angle + 0.001)
+    order = oracle.order_by_distance(d)
+    keys = radix_key(d.astype(np.float32))
+    ref = np.lexsort((np.arange(d.size), keys))
+    assert np.array_equal(order, ref.astype(np.uint32))
+
+
+def test_negative_zero_sorts_before_positive_zero(oracle):
+    d = np.array([0.0, -0.0, 1e-50, -1e-50, 0.0], np.float64)
+    # f32 casts: 0, -0, +0 (underflow), -0 (underflow), 0
+    order = oracle.order_by_distance(d)
+    assert order.tolist() == [1, 3, 0, 2, 4]
+
+
+def test_threads_do_not_change_results(oracle, synth):
+    z = synth.fbm(81, 81, 0.7, 7, 0.0, 300.0)
+    g = oracle.geometry(81, 10.0, 300, 50.0)
+    a = oracle.run(g, z, 1.65, 0, 30, rings=True, threads=1)
+    b = oracle.run(g, z, 1.65, 0, 30, rings=True, threads=6)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+
+
+def test_unfilled_delta_tail(oracle):
+    """band_of_sight.rs:158 fills 2*band_size - band_samples/2 entries of the
+    band_size - 1 table; the rest keep delta 0 and distance 0."""
+    g = oracle.geometry(301, 30.0, 3000)
+    deltas, dists, filled = oracle.compile_band_data(g, 17.0)
+    assert g.band_deltas_size == 100 and filled == 60
+    assert not deltas[filled:].any() and not dists[filled:].any()
+    assert (dists[:filled] > 0).all()
+
+
+def test_los_too_long(oracle):
+    with pytest.raises(oracle.OracleError) as e:
+        oracle.geometry(101, 1.0, 51)
+    assert e.value.code == -2
+
+
+def test_los_too_short_for_shape(oracle):
+    g = oracle.geometry(101, 1.0, 1)  # band_size 2: band_of_sight.rs indexes past the table
+    with pytest.raises(oracle.OracleError) as e:
+        oracle.compile_band_data(g, 0.0)
+    assert e.value.code == -3
+
+
+def test_ring_overflow_past_buffer_end_is_an_error(oracle, synth):
+    z = synth.fbm(301, 301, 0.8, 20261203, 0.0, 1500.0)
+    g = oracle.geometry(301, 30.0, 3000, 5.0)  # 15 slots: the reference panics
+    with pytest.raises(oracle.OracleError) as e:
+        oracle.run(g, z, 1.65, 0, 180, rings=True)
+    assert e.value.code == -5
+
+
+def test_f64_close_to_f32(oracle, synth):
+    z = synth.fbm(61, 61, 0.8, 3, 0.0, 200.0)
+    g = oracle.geometry(61, 5.0, 100)
+    c32, _, _ = oracle.run(g, z, 1.65, 0, 180)
+    c64, _ = oracle.run_f64(g, z, 1.65, 0, 180)
+    rel = np.abs(c32 - c64) / np.maximum(np.abs(c64), 1e-9)
+    assert rel.max() < 5e-3
+    assert np.median(rel) < 1e-5
+
+
+def test_geometry_matches_dem_rs(oracle):
+    """dem.rs:44-82 for the benchmark configurations."""
+    for w, s, los, lp, tvs in [(301, 30.0, 3000, 100, 101), (1201, 90.0, 36000, 400, 401),
+                               (3601, 30.0, 36000, 1200, 1201), (7201, 30.0, 72000, 2400, 2401)]:
+        g = oracle.geometry(w, s, los)
+        assert (g.max_los_as_points, g.tvs_width, g.computable_points_count) == (lp, tvs, tvs * tvs)
+        assert g.band_size == lp + 1 and g.total_bands == 2 * tvs * tvs
+
+
+def test_zero_total_bands_is_fine(oracle):
+    g = oracle.geometry(9, 1.0, 4)
+    z = f32(np.arange(81) % 5)
+    cum, total, _ = oracle.run(g, z, 1.8, 0, 3)
+    assert cum.size == g.computable_points_count

@@ -1,0 +1,386 @@
+"""total-viewsheds_b200: the B200 total-viewshed engine behind a ctypes binding.
+
+This module binds libtvs_cuda.so (include/tvs.h) and mirrors the reference's
+host interface for the hot path, crates/total-viewsheds/src:
+
+    DEM(width, scale, max_line_of_sight)      dem.rs:44-72
+    Compute(method, ..., dem, rings_per_km)   compute.rs:27-84
+    Compute.run() -> (cumulative, rings)      compute.rs:101-115
+    Compute.compute_sector(angle, cum, rings) compute.rs:181-203 (ComputeType::Cuda)
+
+There is no CPU fallback: every compute call goes through the CUDA library and
+raises TvsError when it (or a GPU) is missing.
+"""
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libtvs_cuda.so"
+SECTOR_STEPS = 180
+
+OK = 0
+ERR_INVALID_ARGUMENT = -1
+ERR_LOS_TOO_LONG = -2
+ERR_SHAPE = -3
+ERR_PATH_OUT_OF_DEM = -4
+ERR_RING_OVERFLOW = -5
+ERR_CUDA = -6
+ERR_NO_DEVICE = -7
+ERR_OUT_OF_MEMORY = -8
+ERR_CAPACITY = -9
+ERR_TIMEOUT = -10
+
+PRECISION = {"exact32": 0, "mixed64": 1, "fp64": 2}
+SWEEP_KERNEL = {"engine": 0, "plain": 1}
+
+
+class TvsError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_uint32),
+        ("height", ctypes.c_uint32),
+        ("scale", ctypes.c_float),
+        ("max_line_of_sight", ctypes.c_uint32),
+        ("rings_per_km", ctypes.c_float),
+        ("observer_height", ctypes.c_float),
+        ("precision", ctypes.c_uint32),
+        ("sweep_kernel", ctypes.c_uint32),
+        ("device", ctypes.c_int32),
+        ("tvs_row_begin", ctypes.c_uint32),
+        ("tvs_row_end", ctypes.c_uint32),
+    ]
+
+
+class Geometry(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_uint32),
+        ("height", ctypes.c_uint32),
+        ("max_los_as_points", ctypes.c_uint32),
+        ("band_size", ctypes.c_uint32),
+        ("band_deltas_size", ctypes.c_uint32),
+        ("tvs_width", ctypes.c_uint32),
+        ("tvs_height", ctypes.c_uint32),
+        ("reserved_rings_per_band", ctypes.c_uint32),
+        ("band_samples", ctypes.c_uint32),
+        ("band_steps_filled", ctypes.c_uint32),
+        ("size", ctypes.c_uint64),
+        ("computable_points_count", ctypes.c_uint64),
+        ("total_bands", ctypes.c_uint64),
+        ("ring_slots_per_sector", ctypes.c_uint64),
+    ]
+
+
+class SectorStats(ctypes.Structure):
+    _fields_ = [
+        ("angle", ctypes.c_uint32),
+        ("band_steps_filled", ctypes.c_uint32),
+        ("overflow_bands", ctypes.c_uint32),
+        ("max_ring_ids", ctypes.c_uint32),
+        ("spill_entries", ctypes.c_uint64),
+    ]
+
+
+SECTOR_CALLBACK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32,
+                                   ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint64,
+                                   ctypes.POINTER(SectorStats))
+
+# Every entry point of include/tvs.h with its ctypes signature.
+_VP, _U32, _U64, _I32, _INT = (ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64,
+                               ctypes.c_int32, ctypes.c_int)
+_P = ctypes.POINTER
+SIGNATURES = {
+    "tvs_abi_version": (_INT, []),
+    "tvs_create": (_INT, [_P(Params), _VP, _U64, _P(_VP)]),
+    "tvs_destroy": (None, [_VP]),
+    "tvs_last_error": (ctypes.c_char_p, [_VP]),
+    "tvs_compute_geometry": (_INT, [_P(Params), _P(Geometry)]),
+    "tvs_get_geometry": (_INT, [_VP, _P(Geometry)]),
+    "tvs_set_elevations": (_INT, [_VP, _VP, _U64]),
+    "tvs_axes": (_INT, [_VP, _U32, _U64, _U64, _VP, _VP]),
+    "tvs_band_shape": (_INT, [_VP, _U32, _VP, _VP, _P(_U32)]),
+    "tvs_compute_sector": (_INT, [_VP, _U32, _VP, _VP, _U64, _P(SectorStats)]),
+    "tvs_run": (_INT, [_VP, _VP, _VP, _INT, SECTOR_CALLBACK, _VP]),
+    "tvs_device_reset": (_INT, [_VP]),
+    "tvs_device_run_sectors": (_INT, [_VP, _U32, _U32]),
+    "tvs_device_shape_sectors": (_INT, [_VP, _U32, _U32]),
+    "tvs_device_sweep_sectors": (_INT, [_VP, _U32, _U32]),
+    "tvs_device_finish": (_INT, [_VP]),
+    "tvs_read_surfaces": (_INT, [_VP, _VP, _VP]),
+    "tvs_device_cumulative": (_VP, [_VP]),
+    "tvs_stream": (_VP, [_VP]),
+    "tvs_last_launch_count": (_U64, [_VP]),
+    "tvs_selftest_division": (_INT, [_I32, _U64, _U64, _P(_U64)]),
+    "tvs_measure_fp32_issue": (_INT, [_I32, _P(ctypes.c_double)]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load libtvs_cuda.so; raises when it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise TvsError(ERR_INVALID_ARGUMENT,
+                           f"{LIB_PATH} is missing: build it with total-viewsheds_b200/build.py")
+        L = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _raise(code, ctx=None):
+    msg = lib().tvs_last_error(ctx)
+    raise TvsError(code, msg.decode() if msg else "error")
+
+
+def make_params(width, scale, max_line_of_sight, rings_per_km=5.0, observer_height=1.8,
+                height=None, precision="exact32", sweep_kernel="engine", device=0,
+                rows=None):
+    p = Params()
+    p.width = width
+    p.height = width if height is None else height
+    p.scale = scale
+    p.max_line_of_sight = int(max_line_of_sight)
+    p.rings_per_km = rings_per_km
+    p.observer_height = observer_height
+    p.precision = PRECISION[precision] if isinstance(precision, str) else precision
+    p.sweep_kernel = SWEEP_KERNEL[sweep_kernel] if isinstance(sweep_kernel, str) else sweep_kernel
+    p.device = device
+    p.tvs_row_begin, p.tvs_row_end = (0, 0) if rows is None else rows
+    return p
+
+
+def compute_geometry(params):
+    """DEM::new + Compute::new geometry (no GPU needed)."""
+    g = Geometry()
+    rc = lib().tvs_compute_geometry(ctypes.byref(params), ctypes.byref(g))
+    if rc:
+        _raise(rc)
+    return g
+
+
+class Engine:
+    """One CUDA context (tvs_context) holding a DEM resident in HBM."""
+
+    def __init__(self, elevations, width, scale, max_line_of_sight, **kw):
+        self.params = make_params(width, scale, max_line_of_sight, **kw)
+        e = np.ascontiguousarray(elevations, np.float32).ravel()
+        ctx = ctypes.c_void_p()
+        rc = lib().tvs_create(ctypes.byref(self.params), _ptr(e), e.size, ctypes.byref(ctx))
+        if rc:
+            _raise(rc)
+        self.ctx = ctx
+        self.geometry = Geometry()
+        lib().tvs_get_geometry(self.ctx, ctypes.byref(self.geometry))
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            lib().tvs_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc):
+        if rc:
+            _raise(rc, self.ctx)
+
+    @property
+    def count(self):
+        return self.geometry.computable_points_count
+
+    def set_elevations(self, elevations):
+        e = np.ascontiguousarray(elevations, np.float32).ravel()
+        self._check(lib().tvs_set_elevations(self.ctx, _ptr(e), e.size))
+
+    def axes(self, angle, first_rank=0, count=None, sight_distances=False):
+        """(sector_ordered[first_rank:first_rank+count], f32 sight distances or None)."""
+        n = self.geometry.size
+        count = n - first_rank if count is None else count
+        ids = np.empty(count, np.uint32)
+        d = np.empty(n, np.float32) if sight_distances else None
+        self._check(lib().tvs_axes(self.ctx, angle, first_rank, count, _ptr(ids), _ptr(d)))
+        return ids, d
+
+    def band_shape(self, angle):
+        """(band_deltas i32, band_distances f32, band_steps_filled)."""
+        n = self.geometry.band_deltas_size
+        deltas = np.zeros(max(n, 1), np.int32)
+        dists = np.zeros(max(n, 1), np.float32)
+        filled = ctypes.c_uint32()
+        self._check(lib().tvs_band_shape(self.ctx, angle, _ptr(deltas), _ptr(dists),
+                                         ctypes.byref(filled)))
+        return deltas[:n], dists[:n], filled.value
+
+    def compute_sector(self, angle, cumulative, rings=None):
+        """In place on cumulative (f32 [count]); rings (u32 [ring_slots]) receives the
+        sector's ring records.  Returns SectorStats."""
+        assert cumulative.dtype == np.float32 and cumulative.flags.c_contiguous
+        st = SectorStats()
+        self._check(lib().tvs_compute_sector(self.ctx, angle, _ptr(cumulative), _ptr(rings),
+                                             0 if rings is None else rings.size,
+                                             ctypes.byref(st)))
+        return st
+
+    def run(self, rings=False, on_sector=None):
+        """All 180 sectors.  Returns (cumulative, heatmap total, [rings per sector] or None).
+
+        on_sector(angle, rings_or_None, stats) is called after every sector."""
+        cum = np.empty(self.count, np.float32)
+        total = np.empty(self.count, np.float32)
+        kept = [] if rings else None
+
+        def cb(_user, angle, ptr, n, stats):
+            r = None
+            if ptr:
+                r = np.ctypeslib.as_array(ptr, shape=(n,)).copy()
+                if kept is not None:
+                    kept.append(r)
+            if on_sector is not None:
+                on_sector(angle, r, stats.contents)
+            return 0
+
+        cfn = SECTOR_CALLBACK(cb)
+        self._check(lib().tvs_run(self.ctx, _ptr(cum), _ptr(total), 1 if rings else 0, cfn,
+                                  None))
+        return cum, total, kept
+
+    # device-resident form
+    def device_reset(self):
+        self._check(lib().tvs_device_reset(self.ctx))
+
+    def device_run_sectors(self, first=0, count=SECTOR_STEPS):
+        self._check(lib().tvs_device_run_sectors(self.ctx, first, count))
+
+    def device_shape_sectors(self, first=0, count=SECTOR_STEPS):
+        self._check(lib().tvs_device_shape_sectors(self.ctx, first, count))
+
+    def device_sweep_sectors(self, first=0, count=SECTOR_STEPS):
+        self._check(lib().tvs_device_sweep_sectors(self.ctx, first, count))
+
+    def device_finish(self):
+        self._check(lib().tvs_device_finish(self.ctx))
+
+    def read_surfaces(self):
+        cum = np.empty(self.count, np.float32)
+        total = np.empty(self.count, np.float32)
+        self._check(lib().tvs_read_surfaces(self.ctx, _ptr(cum), _ptr(total)))
+        return cum, total
+
+    def stream(self):
+        return lib().tvs_stream(self.ctx)
+
+    def last_launch_count(self):
+        return lib().tvs_last_launch_count(self.ctx)
+
+
+def selftest_division(n, seed=0, device=0):
+    out = ctypes.c_uint64()
+    rc = lib().tvs_selftest_division(device, n, seed, ctypes.byref(out))
+    if rc:
+        _raise(rc)
+    return out.value
+
+
+def measure_fp32_issue(device=0):
+    """Measured FP32 lane-instructions per second on `device`."""
+    out = ctypes.c_double()
+    rc = lib().tvs_measure_fp32_issue(device, ctypes.byref(out))
+    if rc:
+        _raise(rc)
+    return out.value
+
+
+class DEM:
+    """dem.rs:44-140: geometry of a square (or, as an extension, W x H) DEM."""
+
+    def __init__(self, width, scale, max_line_of_sight, height=None, rings_per_km=5.0):
+        self.width = width
+        self.height = width if height is None else height
+        self.scale = scale
+        self.max_line_of_sight = int(max_line_of_sight)
+        g = compute_geometry(make_params(width, scale, max_line_of_sight,
+                                         rings_per_km=rings_per_km, height=height))
+        self.size = g.size
+        self.max_los_as_points = g.max_los_as_points
+        self.computable_points_count = g.computable_points_count
+        self.tvs_width = g.tvs_width
+        self.tvs_height = g.tvs_height
+        self.band_size = g.band_size
+        self.elevations = np.zeros(self.size, np.float32)
+
+    def band_deltas_size(self):
+        return self.band_size - 1                     # band_of_sight.rs:54-58
+
+    def tvs_id_to_pov_id(self, tvs_id):               # dem.rs:121-127
+        x = tvs_id % self.tvs_width + self.max_los_as_points
+        y = tvs_id // self.tvs_width + self.max_los_as_points
+        return y * self.width + x
+
+    def pov_id_to_tvs_id(self, pov_id):               # dem.rs:110-118
+        x = pov_id % self.width - self.max_los_as_points
+        y = pov_id // self.width - self.max_los_as_points
+        return y * self.tvs_width + x
+
+
+class Compute:
+    """compute.rs:6-241 with the `--compute cuda` backend.
+
+    Only method="cuda" exists here; the reference's CPU and Vulkan arms are
+    not part of this engine.  observer_height defaults to the reference's
+    hard-coded 1.8 m (compute.rs:41)."""
+
+    def __init__(self, method, state_directory, output_dir, dem, rings_per_km,
+                 observer_height=1.8, keep_rings=True, precision="exact32",
+                 sweep_kernel="engine", device=0):
+        if method != "cuda":
+            raise TvsError(ERR_INVALID_ARGUMENT, f"unsupported compute method {method!r}")
+        self.dem = dem
+        self.state_directory = state_directory
+        self.output_dir = output_dir
+        self.keep_rings = keep_rings
+        self.engine = Engine(dem.elevations, dem.width, dem.scale, dem.max_line_of_sight,
+                             height=dem.height, rings_per_km=rings_per_km,
+                             observer_height=observer_height, precision=precision,
+                             sweep_kernel=sweep_kernel, device=device)
+        g = self.engine.geometry
+        self.total_reserved_rings = g.ring_slots_per_sector
+        self.reserved_rings_per_band = g.reserved_rings_per_band
+        self.total_surfaces = np.zeros(g.computable_points_count, np.float32)
+
+    def run(self):
+        """compute.rs:101-115: returns (cumulative_surfaces, all_ring_data)."""
+        cum, total, rings = self.engine.run(rings=self.keep_rings)
+        self.total_surfaces = total
+        return cum, (rings if rings is not None else [])
+
+    def compute_sector(self, angle, cumulative_surfaces, ring_data=None):
+        """compute.rs:181-203 for one sector (in place)."""
+        st = self.engine.compute_sector(angle, cumulative_surfaces, ring_data)
+        self.total_surfaces += cumulative_surfaces          # compute.rs:206-214
+        return st

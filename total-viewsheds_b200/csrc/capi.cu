@@ -1,0 +1,765 @@
+// capi.cu -- the extern "C" boundary (include/tvs.h) and the per-context
+// orchestration of the shape and sweep stages.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "tvs.h"
+#include "tvs_internal.cuh"
+
+struct tvs_context {
+    tvs_params p{};
+    tvs_geometry g{};
+    uint32_t row_begin = 0, row_end = 0;
+    int64_t pov_min = 0, pov_max = 0;
+    uint32_t step_cap = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    uint64_t launches = 0;
+
+    float *d_elev = nullptr;
+    float *d_cum = nullptr;
+    float *d_total = nullptr;
+    double *d_cum64 = nullptr;
+    tvs::SectorTrig *d_trig = nullptr;
+    tvs::ShapeHeader *d_hdr = nullptr;   // [180 + 1]: the last slot serves tvs_axes
+    float4 *d_steps = nullptr;
+    int2 *d_offs = nullptr;
+    int32_t *d_deltas = nullptr;
+    float *d_dists = nullptr;
+    // ring output (allocated on first use)
+    uint32_t *d_rings = nullptr;
+    uint4 *d_spill = nullptr;
+    uint32_t *d_counters = nullptr;
+    uint32_t spill_cap = 0;
+    // plain-kernel scratch (allocated on first use)
+    float *d_sf = nullptr, *d_sb = nullptr;
+    // sectors whose shape stage ran since the last tvs_device_finish
+    bool pending[tvs::kSectorSteps] = {};
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+constexpr double kRadsPerDeg = 3.14159265358979323846 / 180.0;  // Rust f64::to_radians
+constexpr double kSqrt2 = 1.41421356237309504880;               // core::f64::consts::SQRT_2
+constexpr uint32_t kSpillCap = 1u << 20;
+
+int fail(tvs_context *ctx, int code, const std::string &msg) {
+    if (ctx) ctx->err = msg; else g_create_error = msg;
+    return code;
+}
+
+int cuda_fail(tvs_context *ctx, cudaError_t e, const char *what) {
+    return fail(ctx, TVS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define TVS_CUDA(ctx, expr)                                   \
+    do {                                                      \
+        cudaError_t e_ = (expr);                              \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #expr); \
+    } while (0)
+
+// Rust `f32 as u32` (saturating, NaN -> 0).
+uint32_t f32_as_u32(float v) {
+    if (!(v > 0.0f)) return 0;
+    if (v >= 4294967296.0f) return UINT32_MAX;
+    return (uint32_t)v;
+}
+
+// dem.rs:106-115 along one axis (the test is separable for a rectangle).
+uint32_t computable_along(uint32_t extent, float scale, uint32_t los_m) {
+    const float lower = (float)los_m;
+    const float upper = ((float)(extent - 1) * scale) - lower;
+    uint32_t n = 0;
+    for (uint32_t i = 0; i < extent; i++) {
+        const float v = (float)i * scale;
+        if (v >= lower && v <= upper) n++;
+    }
+    return n;
+}
+
+uint64_t isqrt_u64(uint64_t n) {
+    uint64_t r = (uint64_t)std::sqrt((double)n);
+    while (r * r > n) r--;
+    while ((r + 1) * (r + 1) <= n) r++;
+    return r;
+}
+
+// DEM::new (dem.rs:44-72), Compute::new (compute.rs:34-47) and the index
+// ranges compile_band_data relies on (band_of_sight.rs:95-165).  Returns an
+// error where the reference bails or panics.
+int derive_geometry(const tvs_params *p, tvs_geometry *g, std::string *msg) {
+    std::memset(g, 0, sizeof(*g));
+    if (!p || p->width == 0 || p->height == 0) {
+        *msg = "width and height must be positive";
+        return TVS_ERR_INVALID_ARGUMENT;
+    }
+    if (!(p->scale > 0.0f) || !std::isfinite(p->scale)) {
+        *msg = "scale must be a positive finite number of metres";
+        return TVS_ERR_INVALID_ARGUMENT;
+    }
+    g->width = p->width;
+    g->height = p->height;
+    g->size = (uint64_t)p->width * p->height;
+    if (g->size >= (1ull << 31)) {
+        *msg = "DEM ids must fit in i32 (band_of_sight.rs:160)";
+        return TVS_ERR_INVALID_ARGUMENT;
+    }
+    g->max_los_as_points = f32_as_u32((float)p->max_line_of_sight / p->scale);
+    const uint32_t shorter = std::min(p->width, p->height);
+    if (g->max_los_as_points > shorter / 2) {
+        char b[256];
+        std::snprintf(b, sizeof b,
+                      "The maximum line of sight (%um) is longer than the maximum distance "
+                      "that any point can completely see (%gm).",
+                      p->max_line_of_sight, (double)(shorter / 2) * (double)p->scale);
+        *msg = b;
+        return TVS_ERR_LOS_TOO_LONG;
+    }
+    g->band_size = g->max_los_as_points + 1;
+    g->band_deltas_size = g->band_size - 1;
+    const uint32_t nx = computable_along(p->width, p->scale, p->max_line_of_sight);
+    const uint32_t ny = computable_along(p->height, p->scale, p->max_line_of_sight);
+    g->computable_points_count = (uint64_t)nx * ny;
+    if (p->width == p->height) {
+        g->tvs_width = (uint32_t)isqrt_u64(g->computable_points_count);
+        g->tvs_height = g->tvs_width;
+    } else {
+        g->tvs_width = nx;
+        g->tvs_height = ny;
+    }
+    g->total_bands = 2 * g->computable_points_count;
+    const float band_length_in_km = (float)p->max_line_of_sight / 1000.0f;
+    g->reserved_rings_per_band = f32_as_u32(band_length_in_km * p->rings_per_km);
+    g->ring_slots_per_sector = g->total_bands * g->reserved_rings_per_band;
+    const uint64_t bs = (uint64_t)((double)(g->band_size * 2) * kSqrt2);
+    g->band_samples = (uint32_t)bs;
+    const uint64_t middle = bs / 2, end = 2ull * g->band_size;
+    if (bs / 2 > g->size / 2 || g->size / 2 - bs / 2 + bs > g->size || end >= bs ||
+        end - middle > g->band_deltas_size) {
+        *msg = "line of sight too short for the band-of-sight shape (band_of_sight.rs:103-165 "
+               "index out of bounds)";
+        return TVS_ERR_SHAPE;
+    }
+    g->band_steps_filled = (uint32_t)(end - middle);
+    if (bs > tvs::kWindowCap ||
+        (uint64_t)(g->band_deltas_size + 2) * 8 + (uint64_t)g->band_deltas_size * 4 >
+            (uint64_t)tvs::kCandidateCap * 8) {
+        *msg = "band_samples exceeds the shape stage's shared-memory capacity";
+        return TVS_ERR_CAPACITY;
+    }
+    return TVS_OK;
+}
+
+void free_all(tvs_context *c) {
+    void *ptrs[] = {c->d_elev, c->d_cum, c->d_total, c->d_cum64, c->d_trig, c->d_hdr,
+                    c->d_steps, c->d_offs, c->d_deltas, c->d_dists, c->d_rings, c->d_spill,
+                    c->d_counters, c->d_sf, c->d_sb};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+tvs::ShapeArgs shape_args(tvs_context *c, uint32_t first_slot) {
+    tvs::ShapeArgs a{};
+    a.width = c->g.width;
+    a.height = c->g.height;
+    a.size = c->g.size;
+    a.band_size = c->g.band_size;
+    a.band_deltas_size = c->g.band_deltas_size;
+    a.band_samples = c->g.band_samples;
+    a.first_angle = first_slot;
+    a.step_cap = c->step_cap;
+    a.pov_min = c->pov_min;
+    a.pov_max = c->pov_max;
+    a.trig = c->d_trig + first_slot;
+    a.hdr = c->d_hdr + first_slot;
+    a.steps = c->d_steps + (uint64_t)first_slot * c->step_cap;
+    a.offs = c->d_offs + (uint64_t)first_slot * c->step_cap;
+    a.deltas = c->d_deltas + (uint64_t)first_slot * c->g.band_deltas_size;
+    a.dists = c->d_dists + (uint64_t)first_slot * c->g.band_deltas_size;
+    return a;
+}
+
+tvs::SweepArgs sweep_args(tvs_context *c, uint32_t first, uint32_t count) {
+    tvs::SweepArgs a{};
+    a.elev = c->d_elev;
+    a.width = c->g.width;
+    a.tvs_width = c->g.tvs_width;
+    a.row_begin = c->row_begin;
+    a.row_end = c->row_end;
+    a.los = c->g.max_los_as_points;
+    a.observer_height = c->p.observer_height;
+    a.n_sectors = count;
+    a.step_cap = c->step_cap;
+    a.hdr = c->d_hdr + first;
+    a.steps = c->d_steps + (uint64_t)first * c->step_cap;
+    a.offs = c->d_offs + (uint64_t)first * c->step_cap;
+    a.cumulative = c->d_cum;
+    a.total = c->d_total;
+    a.cumulative64 = c->d_cum64;
+    a.reserved = c->g.reserved_rings_per_band;
+    a.half_bands = c->g.computable_points_count;
+    return a;
+}
+
+int ensure_rings(tvs_context *c) {
+    if (c->d_rings) return TVS_OK;
+    if (c->g.ring_slots_per_sector == 0)
+        return fail(c, TVS_ERR_RING_OVERFLOW,
+                    "no ring slots are reserved (rings_per_km * line of sight < 1 slot): the "
+                    "reference's first ring write is out of bounds (kernel.rs:307)");
+    c->spill_cap = kSpillCap;
+    cudaError_t e = cudaMalloc(&c->d_rings, c->g.ring_slots_per_sector * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_spill, (size_t)c->spill_cap * sizeof(uint4));
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_counters, 4 * sizeof(uint32_t));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, e == cudaErrorMemoryAllocation ? TVS_ERR_OUT_OF_MEMORY : TVS_ERR_CUDA,
+                    std::string("ring buffer allocation: ") + cudaGetErrorString(e));
+    }
+    return TVS_OK;
+}
+
+int ensure_plain_scratch(tvs_context *c) {
+    if (c->d_sf) return TVS_OK;
+    const uint64_t n = (uint64_t)(c->row_end - c->row_begin) * c->g.tvs_width;
+    TVS_CUDA(c, cudaMalloc(&c->d_sf, std::max<uint64_t>(n, 1) * sizeof(float)));
+    TVS_CUDA(c, cudaMalloc(&c->d_sb, std::max<uint64_t>(n, 1) * sizeof(float)));
+    return TVS_OK;
+}
+
+int enqueue_shape(tvs_context *c, uint32_t first, uint32_t count) {
+    tvs::ShapeArgs a = shape_args(c, first);
+    TVS_CUDA(c, tvs::launch_shape(a, count, c->stream));
+    c->launches++;
+    for (uint32_t s = first; s < first + count && s < tvs::kSectorSteps; s++) c->pending[s] = true;
+    return TVS_OK;
+}
+
+// Sweep sectors [first, first+count) (slots == angles).  With rings, count is 1.
+int enqueue_sweep(tvs_context *c, uint32_t first, uint32_t count, bool rings) {
+    if (c->p.sweep_kernel == TVS_SWEEP_PLAIN) {
+        int rc = ensure_plain_scratch(c);
+        if (rc) return rc;
+        for (uint32_t s = first; s < first + count; s++) {
+            tvs::PlainArgs a{};
+            a.elev = c->d_elev;
+            a.width = c->g.width;
+            a.tvs_width = c->g.tvs_width;
+            a.los = c->g.max_los_as_points;
+            a.row_begin = c->row_begin;
+            a.row_end = c->row_end;
+            a.observer_height = c->p.observer_height;
+            a.band_deltas_size = c->g.band_deltas_size;
+            a.hdr = c->d_hdr + s;
+            a.deltas = c->d_deltas + (uint64_t)s * c->g.band_deltas_size;
+            a.dists = c->d_dists + (uint64_t)s * c->g.band_deltas_size;
+            a.sf = c->d_sf;
+            a.sb = c->d_sb;
+            a.reserved = c->g.reserved_rings_per_band;
+            a.half_bands = c->g.computable_points_count;
+            if (rings) {
+                a.rings = c->d_rings;
+                a.spill = c->d_spill;
+                a.spill_cap = c->spill_cap;
+                a.counters = c->d_counters;
+            }
+            TVS_CUDA(c, tvs::launch_sweep_plain(a, c->stream));
+            const uint64_t off = (uint64_t)c->row_begin * c->g.tvs_width;
+            const uint64_t n = (uint64_t)(c->row_end - c->row_begin) * c->g.tvs_width;
+            TVS_CUDA(c, tvs::launch_combine(c->d_cum + off, c->d_total + off, c->d_sf, c->d_sb,
+                                            n, c->stream));
+            c->launches += 2;
+        }
+        return TVS_OK;
+    }
+    tvs::SweepArgs a = sweep_args(c, first, count);
+    if (rings) {
+        a.rings = c->d_rings;
+        a.spill = c->d_spill;
+        a.spill_cap = c->spill_cap;
+        a.counters = c->d_counters;
+    }
+    TVS_CUDA(c, tvs::launch_sweep_engine(a, (int)c->p.precision, c->stream));
+    c->launches++;
+    return TVS_OK;
+}
+
+int header_status(tvs_context *c, uint32_t first, uint32_t count) {
+    std::vector<tvs::ShapeHeader> h(count);
+    TVS_CUDA(c, cudaMemcpyAsync(h.data(), c->d_hdr + first, count * sizeof(tvs::ShapeHeader),
+                                cudaMemcpyDeviceToHost, c->stream));
+    TVS_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (uint32_t i = 0; i < count; i++) {
+        if (h[i].status == TVS_OK) continue;
+        char b[256];
+        const char *what = h[i].status == TVS_ERR_PATH_OUT_OF_DEM
+                               ? "a band of sight walks off the DEM (kernel.rs:164 index out of "
+                                 "bounds)"
+                           : h[i].status == TVS_ERR_CAPACITY
+                               ? "too many sector-order key ties for the shape stage"
+                               : "shape stage failed";
+        std::snprintf(b, sizeof b, "sector %u: %s", first + i, what);
+        return fail(c, h[i].status, b);
+    }
+    return TVS_OK;
+}
+
+// Copy one sector's ring records to the host and apply the spilled ids with
+// the reference's sequential semantics: band k writes slots k*R .. k*R+n_k
+// (kernel.rs:141-243), so an id past its own record lands in a later band's
+// record unless that band's own (later) writes cover the slot.
+int collect_rings(tvs_context *c, uint32_t *rings, uint64_t rings_len, tvs_sector_stats *st) {
+    uint32_t cnt[4];
+    TVS_CUDA(c, cudaMemcpyAsync(cnt, c->d_counters, sizeof cnt, cudaMemcpyDeviceToHost,
+                                c->stream));
+    TVS_CUDA(c, cudaMemcpyAsync(rings, c->d_rings, c->g.ring_slots_per_sector * sizeof(uint32_t),
+                                cudaMemcpyDeviceToHost, c->stream));
+    TVS_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (st) {
+        st->overflow_bands = cnt[1];
+        st->max_ring_ids = cnt[2];
+        st->spill_entries = cnt[0];
+    }
+    if (cnt[0] == 0) return TVS_OK;
+    if (cnt[0] > c->spill_cap)
+        return fail(c, TVS_ERR_CAPACITY, "ring spill list capacity exceeded");
+    std::vector<uint4> sp(cnt[0]);
+    TVS_CUDA(c, cudaMemcpy(sp.data(), c->d_spill, cnt[0] * sizeof(uint4), cudaMemcpyDeviceToHost));
+    std::sort(sp.begin(), sp.end(), [](const uint4 &x, const uint4 &y) {
+        uint64_t kx = x.x | ((uint64_t)x.y << 32), ky = y.x | ((uint64_t)y.y << 32);
+        return kx != ky ? kx < ky : x.z < y.z;
+    });
+    const uint64_t R = c->g.reserved_rings_per_band;
+    const uint64_t limit = std::min<uint64_t>(rings_len, c->g.ring_slots_per_sector);
+    for (const uint4 &s : sp) {
+        const uint64_t kid = s.x | ((uint64_t)s.y << 32);
+        const uint64_t at = kid * R + s.z;
+        if (at >= limit) {
+            char b[200];
+            std::snprintf(b, sizeof b,
+                          "ring records overflow the sector buffer (band %llu slot %u; "
+                          "kernel.rs:307 index out of bounds): raise --rings-per-km",
+                          (unsigned long long)kid, s.z);
+            return fail(c, TVS_ERR_RING_OVERFLOW, b);
+        }
+        const uint64_t owner = at / R, q = at % R;
+        if (q > rings[owner * R]) rings[at] = s.w;  // owner's own writes cover 0..n_owner
+    }
+    return TVS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tvs_abi_version(void) { return TVS_ABI_VERSION; }
+
+const char *tvs_last_error(const tvs_context *ctx) {
+    return ctx ? ctx->err.c_str() : g_create_error.c_str();
+}
+
+int tvs_compute_geometry(const tvs_params *params, tvs_geometry *out) {
+    if (!params || !out) return fail(nullptr, TVS_ERR_INVALID_ARGUMENT, "null argument");
+    std::string msg;
+    int rc = derive_geometry(params, out, &msg);
+    if (rc) return fail(nullptr, rc, msg);
+    return TVS_OK;
+}
+
+int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_elevations,
+               tvs_context **out) {
+    if (!params || !out) return fail(nullptr, TVS_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    tvs_geometry g;
+    std::string msg;
+    int rc = derive_geometry(params, &g, &msg);
+    if (rc) return fail(nullptr, rc, msg);
+    if (!elevations || n_elevations != g.size)
+        return fail(nullptr, TVS_ERR_INVALID_ARGUMENT, "elevations must hold width*height values");
+    if (params->precision > TVS_PRECISION_FP64 || params->sweep_kernel > TVS_SWEEP_PLAIN ||
+        (params->sweep_kernel == TVS_SWEEP_PLAIN && params->precision != TVS_PRECISION_EXACT32))
+        return fail(nullptr, TVS_ERR_INVALID_ARGUMENT, "unsupported precision/sweep-kernel pair");
+    if (params->precision == TVS_PRECISION_MIXED64)
+        return fail(nullptr, TVS_ERR_INVALID_ARGUMENT, "MIXED64 precision is not available yet");
+    uint32_t rb = params->tvs_row_begin, re = params->tvs_row_end;
+    if (rb == 0 && re == 0) re = g.tvs_height;
+    if (rb > re || re > g.tvs_height)
+        return fail(nullptr, TVS_ERR_INVALID_ARGUMENT, "tvs row range outside the computable grid");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(nullptr, TVS_ERR_NO_DEVICE, "no CUDA device");
+    }
+    if (params->device < 0 || params->device >= ndev)
+        return fail(nullptr, TVS_ERR_NO_DEVICE, "device ordinal out of range");
+
+    tvs_context *c = new tvs_context();
+    c->p = *params;
+    c->g = g;
+    c->row_begin = rb;
+    c->row_end = re;
+    const uint64_t los = g.max_los_as_points;
+    if (g.computable_points_count) {
+        c->pov_min = (int64_t)(los * g.width + los);
+        c->pov_max = (int64_t)((g.tvs_height - 1 + los) * g.width + (g.tvs_width - 1 + los));
+    }
+    c->step_cap = (g.band_steps_filled + 2 + 3) & ~3u;
+    auto bail = [&](cudaError_t e, const char *what) {
+        std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+        int code = e == cudaErrorMemoryAllocation ? TVS_ERR_OUT_OF_MEMORY : TVS_ERR_CUDA;
+        cudaGetLastError();
+        free_all(c);
+        delete c;
+        return fail(nullptr, code, m);
+    };
+    cudaError_t e = cudaSetDevice(params->device);
+    if (e != cudaSuccess) return bail(e, "cudaSetDevice");
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail(e, "cudaStreamCreate");
+    const uint64_t count = std::max<uint64_t>(g.computable_points_count, 1);
+    const uint32_t slots = tvs::kSectorSteps + 1;
+    const uint64_t bds = std::max<uint32_t>(g.band_deltas_size, 1);
+    struct { void **p; size_t bytes; } allocs[] = {
+        {(void **)&c->d_elev, g.size * sizeof(float)},
+        {(void **)&c->d_cum, count * sizeof(float)},
+        {(void **)&c->d_total, count * sizeof(float)},
+        {(void **)&c->d_trig, slots * sizeof(tvs::SectorTrig)},
+        {(void **)&c->d_hdr, slots * sizeof(tvs::ShapeHeader)},
+        {(void **)&c->d_steps, (size_t)slots * c->step_cap * sizeof(float4)},
+        {(void **)&c->d_offs, (size_t)slots * c->step_cap * sizeof(int2)},
+        {(void **)&c->d_deltas, (size_t)slots * bds * sizeof(int32_t)},
+        {(void **)&c->d_dists, (size_t)slots * bds * sizeof(float)},
+    };
+    for (auto &a : allocs)
+        if ((e = cudaMalloc(a.p, a.bytes)) != cudaSuccess) return bail(e, "cudaMalloc");
+    if (params->precision == TVS_PRECISION_FP64 &&
+        (e = cudaMalloc(&c->d_cum64, count * sizeof(double))) != cudaSuccess)
+        return bail(e, "cudaMalloc");
+    // Per-sector trigonometry on the host (glibc, as Rust std on linux-gnu):
+    // axes.rs:95 shifts the angle in f32, axes.rs:127 adds 90 in f32.
+    std::vector<tvs::SectorTrig> trig(slots);
+    for (uint32_t s = 0; s < tvs::kSectorSteps; s++) {
+        const float sight = (float)s + tvs::kSectorShift;
+        const float sector = sight + 90.0f;
+        trig[s].sight_sin = std::sin((double)sight * kRadsPerDeg);
+        trig[s].sight_cos = std::cos((double)sight * kRadsPerDeg);
+        trig[s].sector_sin = std::sin((double)sector * kRadsPerDeg);
+        trig[s].sector_cos = std::cos((double)sector * kRadsPerDeg);
+    }
+    trig[tvs::kSectorSteps] = trig[0];
+    if ((e = cudaMemcpy(c->d_trig, trig.data(), slots * sizeof(tvs::SectorTrig),
+                        cudaMemcpyHostToDevice)) != cudaSuccess)
+        return bail(e, "cudaMemcpy trig");
+    if ((e = cudaMemcpy(c->d_elev, elevations, g.size * sizeof(float), cudaMemcpyHostToDevice)) !=
+        cudaSuccess)
+        return bail(e, "cudaMemcpy elevations");
+    if ((e = cudaMemset(c->d_hdr, 0, slots * sizeof(tvs::ShapeHeader))) != cudaSuccess ||
+        (e = cudaMemset(c->d_cum, 0, count * sizeof(float))) != cudaSuccess ||
+        (e = cudaMemset(c->d_total, 0, count * sizeof(float))) != cudaSuccess)
+        return bail(e, "cudaMemset");
+    if (c->d_cum64 && (e = cudaMemset(c->d_cum64, 0, count * sizeof(double))) != cudaSuccess)
+        return bail(e, "cudaMemset");
+    *out = c;
+    return TVS_OK;
+}
+
+void tvs_destroy(tvs_context *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->p.device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    free_all(ctx);
+    delete ctx;
+}
+
+int tvs_get_geometry(const tvs_context *ctx, tvs_geometry *out) {
+    if (!ctx || !out) return TVS_ERR_INVALID_ARGUMENT;
+    *out = ctx->g;
+    return TVS_OK;
+}
+
+int tvs_set_elevations(tvs_context *ctx, const float *elevations, uint64_t n) {
+    if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
+    if (!elevations || n != ctx->g.size)
+        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "elevations must hold width*height values");
+    TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
+    TVS_CUDA(ctx, cudaMemcpyAsync(ctx->d_elev, elevations, n * sizeof(float),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    return TVS_OK;
+}
+
+int tvs_axes(tvs_context *ctx, uint32_t angle, uint64_t first_rank, uint64_t count,
+             uint32_t *sector_ordered, float *sight_distances) {
+    if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
+    if (angle >= tvs::kSectorSteps || first_rank + count > ctx->g.size)
+        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "angle or rank range out of bounds");
+    TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
+    if (sector_ordered && count) {
+        if (count > tvs::kCandidateCap)
+            return fail(ctx, TVS_ERR_CAPACITY, "tvs_axes rank range exceeds the candidate capacity");
+        uint32_t *d_ids = nullptr;
+        TVS_CUDA(ctx, cudaMalloc(&d_ids, count * sizeof(uint32_t)));
+        const uint32_t slot = tvs::kSectorSteps;  // scratch slot
+        tvs::SectorTrig t;
+        TVS_CUDA(ctx, cudaMemcpyAsync(&t, ctx->d_trig + angle, sizeof t, cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+        TVS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        TVS_CUDA(ctx, cudaMemcpyAsync(ctx->d_trig + slot, &t, sizeof t, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+        tvs::ShapeArgs a = shape_args(ctx, slot);
+        a.sector_ids_out = d_ids;
+        a.dbg_first = first_rank;
+        a.dbg_count = count;
+        cudaError_t e = tvs::launch_shape(a, 1, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(sector_ordered, d_ids, count * sizeof(uint32_t),
+                                cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        cudaFree(d_ids);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "tvs_axes");
+        int rc = header_status(ctx, slot, 1);
+        if (rc) return rc;
+    }
+    if (sight_distances) {
+        tvs::SectorTrig t;
+        TVS_CUDA(ctx, cudaMemcpy(&t, ctx->d_trig + angle, sizeof t, cudaMemcpyDeviceToHost));
+        // The same device projection the shape stage uses (axes.rs:154-189).
+        float *d_out = nullptr;
+        TVS_CUDA(ctx, cudaMalloc(&d_out, ctx->g.size * sizeof(float)));
+        cudaError_t e = tvs::launch_sight_distances(t, ctx->g.width, ctx->g.height, d_out,
+                                                    ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(sight_distances, d_out, ctx->g.size * sizeof(float),
+                                cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        cudaFree(d_out);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "tvs_axes sight distances");
+    }
+    return TVS_OK;
+}
+
+int tvs_band_shape(tvs_context *ctx, uint32_t angle, int32_t *band_deltas, float *band_distances,
+                   uint32_t *band_steps_filled) {
+    if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
+    if (angle >= tvs::kSectorSteps) return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "angle >= 180");
+    TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
+    int rc = enqueue_shape(ctx, angle, 1);
+    if (rc) return rc;
+    const uint64_t bds = ctx->g.band_deltas_size;
+    if (band_deltas && bds)
+        TVS_CUDA(ctx, cudaMemcpyAsync(band_deltas, ctx->d_deltas + angle * bds,
+                                      bds * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    if (band_distances && bds)
+        TVS_CUDA(ctx, cudaMemcpyAsync(band_distances, ctx->d_dists + angle * bds,
+                                      bds * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    tvs::ShapeHeader h;
+    TVS_CUDA(ctx, cudaMemcpyAsync(&h, ctx->d_hdr + angle, sizeof h, cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    TVS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (band_steps_filled) *band_steps_filled = h.n_filled;
+    if (h.status == TVS_ERR_CAPACITY || h.status == TVS_ERR_SHAPE) return header_status(ctx, angle, 1);
+    return TVS_OK;
+}
+
+int tvs_compute_sector(tvs_context *ctx, uint32_t angle, float *cumulative_surfaces,
+                       uint32_t *rings, uint64_t rings_len, tvs_sector_stats *stats) {
+    if (!ctx || !cumulative_surfaces) return TVS_ERR_INVALID_ARGUMENT;
+    if (angle >= tvs::kSectorSteps) return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "angle >= 180");
+    if (rings && rings_len < ctx->g.ring_slots_per_sector)
+        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "rings_len is smaller than one sector's slots");
+    TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
+    const uint64_t count = ctx->g.computable_points_count;
+    if (ctx->p.precision == TVS_PRECISION_FP64)
+        return fail(ctx, TVS_ERR_INVALID_ARGUMENT,
+                    "tvs_compute_sector keeps f32 cumulative surfaces; use tvs_run for FP64");
+    if (count)
+        TVS_CUDA(ctx, cudaMemcpyAsync(ctx->d_cum, cumulative_surfaces, count * sizeof(float),
+                                      cudaMemcpyHostToDevice, ctx->stream));
+    if (rings) {
+        int rc = ensure_rings(ctx);
+        if (rc) return rc;
+        TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_rings, 0,
+                                      ctx->g.ring_slots_per_sector * sizeof(uint32_t), ctx->stream));
+        TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), ctx->stream));
+    }
+    int rc = enqueue_shape(ctx, angle, 1);
+    if (rc) return rc;
+    rc = header_status(ctx, angle, 1);
+    if (rc) return rc;
+    rc = enqueue_sweep(ctx, angle, 1, rings != nullptr);
+    if (rc) return rc;
+    if (count)
+        TVS_CUDA(ctx, cudaMemcpyAsync(cumulative_surfaces, ctx->d_cum, count * sizeof(float),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+    if (stats) {
+        std::memset(stats, 0, sizeof *stats);
+        stats->angle = angle;
+        stats->band_steps_filled = ctx->g.band_steps_filled;
+    }
+    if (rings) {
+        rc = collect_rings(ctx, rings, rings_len, stats);
+        if (rc) return rc;
+    }
+    TVS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return TVS_OK;
+}
+
+int tvs_device_reset(tvs_context *ctx) {
+    if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
+    TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
+    const uint64_t count = std::max<uint64_t>(ctx->g.computable_points_count, 1);
+    TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_cum, 0, count * sizeof(float), ctx->stream));
+    TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_total, 0, count * sizeof(float), ctx->stream));
+    if (ctx->d_cum64)
+        TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_cum64, 0, count * sizeof(double), ctx->stream));
+    return TVS_OK;
+}
+
+int tvs_device_shape_sectors(tvs_context *ctx, uint32_t first_angle, uint32_t count) {
+    if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
+    if (first_angle + count > tvs::kSectorSteps)
+        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "sector range beyond 180");
+    if (count == 0) return TVS_OK;
+    TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
+    return enqueue_shape(ctx, first_angle, count);
+}
+
+int tvs_device_sweep_sectors(tvs_context *ctx, uint32_t first_angle, uint32_t count) {
+    if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
+    if (first_angle + count > tvs::kSectorSteps)
+        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "sector range beyond 180");
+    if (count == 0) return TVS_OK;
+    for (uint32_t s = first_angle; s < first_angle + count; s++)
+        if (!ctx->pending[s])
+            return fail(ctx, TVS_ERR_INVALID_ARGUMENT,
+                        "sweep of a sector whose shape stage has not run");
+    TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
+    return enqueue_sweep(ctx, first_angle, count, false);
+}
+
+int tvs_device_run_sectors(tvs_context *ctx, uint32_t first_angle, uint32_t count) {
+    if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
+    ctx->launches = 0;
+    int rc = tvs_device_shape_sectors(ctx, first_angle, count);
+    if (rc) return rc;
+    return tvs_device_sweep_sectors(ctx, first_angle, count);
+}
+
+int tvs_device_finish(tvs_context *ctx) {
+    if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
+    TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
+    TVS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    int rc = TVS_OK;
+    for (uint32_t s = 0; s < tvs::kSectorSteps && rc == TVS_OK; s++) {
+        if (!ctx->pending[s]) continue;
+        uint32_t e = s;
+        while (e < tvs::kSectorSteps && ctx->pending[e]) e++;
+        rc = header_status(ctx, s, e - s);
+        s = e - 1;
+    }
+    for (bool &p : ctx->pending) p = false;
+    return rc;
+}
+
+int tvs_read_surfaces(tvs_context *ctx, float *cumulative_out, float *total_out) {
+    if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
+    TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
+    const uint64_t count = ctx->g.computable_points_count;
+    if (cumulative_out && count)
+        TVS_CUDA(ctx, cudaMemcpyAsync(cumulative_out, ctx->d_cum, count * sizeof(float),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+    if (total_out && count)
+        TVS_CUDA(ctx, cudaMemcpyAsync(total_out, ctx->d_total, count * sizeof(float),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+    TVS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return TVS_OK;
+}
+
+const float *tvs_device_cumulative(const tvs_context *ctx) { return ctx ? ctx->d_cum : nullptr; }
+
+void *tvs_stream(const tvs_context *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+uint64_t tvs_last_launch_count(const tvs_context *ctx) { return ctx ? ctx->launches : 0; }
+
+int tvs_run(tvs_context *ctx, float *cumulative_out, float *total_out, int want_rings,
+            tvs_sector_callback callback, void *user) {
+    if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
+    int rc = tvs_device_reset(ctx);
+    if (rc) return rc;
+    if (!want_rings) {
+        rc = tvs_device_run_sectors(ctx, 0, tvs::kSectorSteps);
+        if (rc) return rc;
+        rc = tvs_device_finish(ctx);
+        if (rc) return rc;
+        if (callback)
+            for (uint32_t s = 0; s < tvs::kSectorSteps; s++) {
+                tvs_sector_stats st{};
+                st.angle = s;
+                st.band_steps_filled = ctx->g.band_steps_filled;
+                if (callback(user, s, nullptr, 0, &st)) break;
+            }
+        return tvs_read_surfaces(ctx, cumulative_out, total_out);
+    }
+    if (ctx->p.precision == TVS_PRECISION_FP64 && !ctx->d_cum64)
+        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "FP64 context without FP64 accumulator");
+    rc = ensure_rings(ctx);
+    if (rc) return rc;
+    std::vector<uint32_t> host_rings(ctx->g.ring_slots_per_sector);
+    for (uint32_t s = 0; s < tvs::kSectorSteps; s++) {
+        TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_rings, 0,
+                                      ctx->g.ring_slots_per_sector * sizeof(uint32_t), ctx->stream));
+        TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), ctx->stream));
+        rc = enqueue_shape(ctx, s, 1);
+        if (rc) return rc;
+        rc = header_status(ctx, s, 1);
+        if (rc) return rc;
+        rc = enqueue_sweep(ctx, s, 1, true);
+        if (rc) return rc;
+        tvs_sector_stats st{};
+        st.angle = s;
+        st.band_steps_filled = ctx->g.band_steps_filled;
+        rc = collect_rings(ctx, host_rings.data(), host_rings.size(), &st);
+        if (rc) return rc;
+        if (callback && callback(user, s, host_rings.data(), host_rings.size(), &st)) break;
+    }
+    return tvs_read_surfaces(ctx, cumulative_out, total_out);
+}
+
+int tvs_selftest_division(int32_t device, uint64_t n, uint64_t seed, uint64_t *mismatches) {
+    if (!mismatches) return fail(nullptr, TVS_ERR_INVALID_ARGUMENT, "null argument");
+    cudaError_t e = cudaSetDevice(device);
+    unsigned long long *d = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&d, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(d, 0, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = tvs::launch_selftest_division(n, seed, d, 0);
+    unsigned long long h = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof h, cudaMemcpyDeviceToHost);
+    if (d) cudaFree(d);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(nullptr, TVS_ERR_CUDA, std::string("selftest: ") + cudaGetErrorString(e));
+    }
+    *mismatches = h;
+    return TVS_OK;
+}
+
+int tvs_measure_fp32_issue(int32_t device, double *instructions_per_second) {
+    if (!instructions_per_second) return fail(nullptr, TVS_ERR_INVALID_ARGUMENT, "null argument");
+    cudaError_t e = cudaSetDevice(device);
+    double v = 0.0;
+    if (e == cudaSuccess) e = tvs::measure_fp32_issue(&v);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(nullptr, TVS_ERR_CUDA, std::string("fp32 issue: ") + cudaGetErrorString(e));
+    }
+    *instructions_per_second = v;
+    return TVS_OK;
+}
+
+}  // extern "C"

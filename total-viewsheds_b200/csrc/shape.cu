@@ -1,0 +1,349 @@
+// shape.cu -- per-sector band-of-sight shape stage (one CTA per sector).
+//
+// Reference: Axes::compute (axes.rs:103-130) sorts all W*H points twice per
+// sector (FP64 projection, f32 cast, stable radix sort) and
+// DEM::compile_band_data (band_of_sight.rs:61-174) then reads only a window of
+// band_samples ranks around the DEM centre from the sector order, re-ordered
+// by sight rank.  This kernel produces exactly that window without a full sort:
+//
+//  1. Along one DEM row the sector projection x*sin - y*cos is monotone in x,
+//     and so are its f32 cast and radix key.  The number of points with key < K
+//     is therefore a sum of per-row binary searches (H * log2(W) evaluations
+//     instead of W*H).
+//  2. A binary search over the 32-bit key space finds the keys K_lo, K_hi of
+//     the first and last window ranks, and count(key < K_lo).
+//  3. The points with K_lo <= key <= K_hi (the window plus key ties) are
+//     gathered into shared memory and sorted by (key, id): radsort is stable,
+//     so this is exactly the reference's sector order on those ranks.
+//  4. The window is sorted by (sight key, id), which orders it by
+//     sight_ordered_map rank (band_of_sight.rs:135-145), and the delta and
+//     distance tables are derived from the strip (band_of_sight.rs:149-170).
+//  5. The sweep's per-step tables (forward offsets, 1/d, d/R, d*tan1) follow.
+//
+// Every projection is rounded op by op (__dmul_rn/__dsub_rn), with host glibc
+// sin/cos, so keys are bitwise those of the reference.
+#include "tvs.h"
+#include "tvs_internal.cuh"
+
+namespace tvs {
+namespace {
+
+// axes.rs:160-171: y runs 0, -1, ..., -(H-1) (row 0 gives +0.0).
+__device__ __forceinline__ double row_term(uint32_t row, double c) {
+    return __dmul_rn((double)(-(int64_t)row), c);
+}
+
+__device__ __forceinline__ float projection32(uint32_t x, double right, double s) {
+    return __double2float_rn(__dsub_rn(__dmul_rn((double)x, s), right));
+}
+
+__device__ __forceinline__ uint32_t key_at(uint32_t x, double right, double s) {
+    return f32_radix_key(projection32(x, right, s));
+}
+
+// Number of x in [0, W) whose key is < K.  Keys are non-decreasing in x when
+// s >= 0 and non-increasing when s < 0.
+__device__ uint32_t row_count_less(uint64_t K, double right, double s, uint32_t W) {
+    uint32_t lo = 0, hi = W;
+    if (!(s < 0.0)) {
+        while (lo < hi) {
+            uint32_t mid = (lo + hi) >> 1;
+            if ((uint64_t)key_at(mid, right, s) < K) lo = mid + 1; else hi = mid;
+        }
+        return lo;
+    }
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if ((uint64_t)key_at(mid, right, s) < K) hi = mid; else lo = mid + 1;
+    }
+    return W - lo;
+}
+
+template <typename T>
+__device__ T block_sum(T v, T *scratch) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    T r = 0;
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int w = 0; w < nw; w++) r += scratch[w];
+    return r;
+}
+
+// Sum over all rows of count(key < K) for two thresholds at once.
+__device__ void count_less2(uint64_t K0, uint64_t K1, double c, double s, uint32_t W,
+                            uint32_t H, uint64_t *out0, uint64_t *out1,
+                            unsigned long long *scratch) {
+    unsigned long long a = 0, b = 0;
+    for (uint32_t row = threadIdx.x; row < H; row += blockDim.x) {
+        double right = row_term(row, c);
+        a += row_count_less(K0, right, s, W);
+        b += row_count_less(K1, right, s, W);
+    }
+    *out0 = block_sum(a, scratch);
+    *out1 = block_sum(b, scratch + 32);
+}
+
+__device__ void bitonic_sort(unsigned long long *v, uint32_t n_pow2) {
+    for (uint32_t k = 2; k <= n_pow2; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < n_pow2; i += blockDim.x) {
+                uint32_t ixj = i ^ j;
+                if (ixj > i) {
+                    unsigned long long a = v[i], b = v[ixj];
+                    bool up = (i & k) == 0;
+                    if ((a > b) == up) { v[i] = b; v[ixj] = a; }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t next_pow2(uint32_t n) {
+    uint32_t p = 1;
+    while (p < n) p <<= 1;
+    return p;
+}
+
+// Inclusive prefix sum of n int64 values in place (one CTA).
+__device__ void block_inclusive_scan(long long *v, uint32_t n, long long *scratch) {
+    const uint32_t T = blockDim.x;
+    const uint32_t per = (n + T - 1) / T;
+    const uint32_t b = threadIdx.x * per;
+    const uint32_t e = min(n, b + per);
+    long long local = 0;
+    for (uint32_t i = b; i < e; i++) local += v[i];
+    // exclusive scan of the per-thread sums through shared memory
+    __syncthreads();
+    scratch[threadIdx.x] = local;
+    __syncthreads();
+    for (uint32_t off = 1; off < T; off <<= 1) {
+        long long add = threadIdx.x >= off ? scratch[threadIdx.x - off] : 0;
+        __syncthreads();
+        scratch[threadIdx.x] += add;
+        __syncthreads();
+    }
+    long long run = scratch[threadIdx.x] - local;
+    for (uint32_t i = b; i < e; i++) { run += v[i]; v[i] = run; }
+    __syncthreads();
+}
+
+struct ShapeSmem {
+    unsigned long long red[64];
+    long long scan[kShapeThreads];
+    uint32_t n_cand;
+    int32_t status;
+};
+
+}  // namespace
+
+__global__ void __launch_bounds__(kShapeThreads, 1)
+k_shape(ShapeArgs a, uint64_t rank_lo, uint64_t rank_count, int axes_mode) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ShapeSmem &sm = *reinterpret_cast<ShapeSmem *>(smem_raw);
+    unsigned long long *cand = reinterpret_cast<unsigned long long *>(smem_raw + sizeof(ShapeSmem));
+    unsigned long long *win = cand + kCandidateCap;
+
+    const uint32_t sector = blockIdx.x;
+    const SectorTrig tr = a.trig[sector];
+    const uint32_t W = a.width, H = a.height;
+    const uint64_t rank_hi = rank_lo + rank_count - 1;
+
+    // 1-2. Keys of ranks rank_lo and rank_hi in the sector order.
+    uint64_t lo0 = 0, hi0 = 0xFFFFFFFFull, lo1 = 0, hi1 = 0xFFFFFFFFull;
+    for (int it = 0; it < 33 && (lo0 < hi0 || lo1 < hi1); it++) {
+        uint64_t mid0 = lo0 + ((hi0 - lo0) >> 1);
+        uint64_t mid1 = lo1 + ((hi1 - lo1) >> 1);
+        uint64_t c0, c1;
+        count_less2(mid0 + 1, mid1 + 1, tr.sector_cos, tr.sector_sin, W, H, &c0, &c1, sm.red);
+        if (lo0 < hi0) { if (c0 > rank_lo) hi0 = mid0; else lo0 = mid0 + 1; }
+        if (lo1 < hi1) { if (c1 > rank_hi) hi1 = mid1; else lo1 = mid1 + 1; }
+    }
+    const uint64_t K_lo = lo0, K_hi = lo1;
+    uint64_t less_lo, le_hi;
+    count_less2(K_lo, K_hi + 1, tr.sector_cos, tr.sector_sin, W, H, &less_lo, &le_hi, sm.red);
+
+    // 3. Gather the candidates (every point with K_lo <= key <= K_hi).
+    if (threadIdx.x == 0) { sm.n_cand = 0; sm.status = TVS_OK; }
+    __syncthreads();
+    const bool inc = !(tr.sector_sin < 0.0);
+    for (uint32_t row = threadIdx.x; row < H; row += blockDim.x) {
+        double right = row_term(row, tr.sector_cos);
+        uint32_t b = row_count_less(K_lo, right, tr.sector_sin, W);
+        uint32_t e = row_count_less(K_hi + 1, right, tr.sector_sin, W);
+        if (e <= b) continue;
+        uint32_t x0 = inc ? b : W - e;
+        uint32_t n = e - b;
+        uint32_t at = atomicAdd(&sm.n_cand, n);
+        for (uint32_t k = 0; k < n; k++) {
+            if (at + k >= kCandidateCap) break;
+            uint32_t x = x0 + k;
+            uint32_t id = row * W + x;
+            cand[at + k] = ((unsigned long long)key_at(x, right, tr.sector_sin) << 32) | id;
+        }
+    }
+    __syncthreads();
+    const uint32_t n_cand = sm.n_cand;
+    ShapeHeader *hdr = a.hdr + sector;
+    if (n_cand > kCandidateCap || less_lo > rank_lo ||
+        (rank_lo - less_lo) + rank_count > n_cand) {
+        if (threadIdx.x == 0) {
+            hdr->status = n_cand > kCandidateCap ? TVS_ERR_CAPACITY : TVS_ERR_SHAPE;
+            hdr->n_candidates = n_cand;
+            hdr->n_filled = hdr->n_steps = 0;
+        }
+        return;
+    }
+    const uint32_t pc = next_pow2(n_cand);
+    for (uint32_t i = n_cand + threadIdx.x; i < pc; i += blockDim.x) cand[i] = ~0ull;
+    __syncthreads();
+    bitonic_sort(cand, pc);
+    const uint32_t start = (uint32_t)(rank_lo - less_lo);
+
+    if (axes_mode) {
+        for (uint32_t j = threadIdx.x; j < rank_count; j += blockDim.x)
+            a.sector_ids_out[j] = (uint32_t)cand[start + j];
+        if (threadIdx.x == 0) { hdr->status = TVS_OK; hdr->n_candidates = n_cand; }
+        return;
+    }
+
+    // 4. Order the window by sight rank == (sight key, id).
+    const uint32_t bs = a.band_samples;
+    for (uint32_t j = threadIdx.x; j < bs; j += blockDim.x) {
+        uint32_t id = (uint32_t)cand[start + j];
+        uint32_t row = id / W, x = id - row * W;
+        float d = projection32(x, row_term(row, tr.sight_cos), tr.sight_sin);
+        win[j] = ((unsigned long long)f32_radix_key(d) << 32) | id;
+    }
+    const uint32_t pw = next_pow2(bs);
+    for (uint32_t i = bs + threadIdx.x; i < pw; i += blockDim.x) win[i] = ~0ull;
+    __syncthreads();
+    bitonic_sort(win, pw);
+
+    // band_of_sight.rs:149-170 (the geometry checks on the host guarantee
+    // middle < end <= band_samples - 1 and filled <= band_deltas_size).
+    const uint32_t middle = bs / 2;
+    const uint32_t n_filled = 2 * a.band_size - middle;
+    const uint32_t bds = a.band_deltas_size;
+    const uint32_t n_steps = n_filled + min(bds - n_filled, 2u);
+    long long *soff = reinterpret_cast<long long *>(cand);           // reuse candidates
+    float *sdist = reinterpret_cast<float *>(soff + bds + 2);
+    const uint32_t pov_id = (uint32_t)(a.size / 2);
+    const float pov_distance =
+        projection32(pov_id % W, row_term(pov_id / W, tr.sight_cos), tr.sight_sin);
+    int32_t *gdel = a.deltas + (uint64_t)sector * bds;
+    float *gdist = a.dists + (uint64_t)sector * bds;
+    for (uint32_t i = threadIdx.x; i < bds; i += blockDim.x) {
+        int32_t delta = 0;
+        float dist = 0.0f;
+        if (i < n_filled) {
+            uint32_t cur = (uint32_t)win[middle + i];
+            uint32_t nxt = (uint32_t)win[middle + i + 1];
+            delta = (int32_t)cur - (int32_t)nxt;
+            uint32_t row = nxt / W, x = nxt - row * W;
+            float nd = projection32(x, row_term(row, tr.sight_cos), tr.sight_sin);
+            dist = fabsf(__fsub_rn(pov_distance, nd));
+        }
+        gdel[i] = delta;
+        gdist[i] = dist;
+        if (i < n_filled) { soff[i] = delta; sdist[i] = dist; }
+    }
+    __syncthreads();
+    block_inclusive_scan(soff, n_filled, sm.scan);
+
+    // 5. Step tables: steps past n_filled repeat the last offset with d = 0.
+    long long mn = 0, mx = 0;
+    float4 *gsteps = a.steps + (uint64_t)sector * a.step_cap;
+    int2 *goffs = a.offs + (uint64_t)sector * a.step_cap;
+    for (uint32_t i = threadIdx.x; i < n_steps; i += blockDim.x) {
+        long long off = i < n_filled ? soff[i] : (n_filled ? soff[n_filled - 1] : 0);
+        float d = i < n_filled ? sdist[i] : 0.0f;
+        float4 st;
+        st.x = __frcp_rn(d);
+        st.y = d;
+        st.z = __fdiv_rn(d, kEarthRadiusSquared);
+        st.w = __fmul_rn(d, kTanOneRad);
+        int flags = (d >= 0x1p-20f && d <= 0x1p20f) ? 0 : kStepSlowDivide;
+        gsteps[i] = st;
+        goffs[i] = make_int2((int32_t)off, flags);
+        mn = min(mn, off);
+        mx = max(mx, off);
+    }
+    __syncthreads();
+    // block min / max through the scan scratch
+    sm.scan[threadIdx.x] = mn;
+    __syncthreads();
+    for (uint32_t o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sm.scan[threadIdx.x] = min(sm.scan[threadIdx.x], sm.scan[threadIdx.x + o]);
+        __syncthreads();
+    }
+    const long long min_off = sm.scan[0];
+    __syncthreads();
+    sm.scan[threadIdx.x] = mx;
+    __syncthreads();
+    for (uint32_t o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sm.scan[threadIdx.x] = max(sm.scan[threadIdx.x], sm.scan[threadIdx.x + o]);
+        __syncthreads();
+    }
+    const long long max_off = sm.scan[0];
+    if (threadIdx.x == 0) {
+        // kernel.rs:157-164: every band of every point of view stays on the DEM.
+        const long long size = (long long)a.size;
+        bool ok = a.pov_min + min_off >= 0 && a.pov_max + max_off < size &&
+                  a.pov_min - max_off >= 0 && a.pov_max - min_off < size &&
+                  min_off >= INT32_MIN && max_off <= INT32_MAX;
+        hdr->status = ok ? TVS_OK : TVS_ERR_PATH_OUT_OF_DEM;
+        hdr->n_filled = n_filled;
+        hdr->n_steps = n_steps;
+        hdr->n_candidates = n_cand;
+        hdr->min_off = min_off;
+        hdr->max_off = max_off;
+    }
+}
+
+// axes.rs:154-189: the f32 sight distance of every point.
+__global__ void k_sight_distances(SectorTrig t, uint32_t W, uint32_t H, float *out) {
+    const uint64_t n = (uint64_t)W * H;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t row = (uint32_t)(i / W), x = (uint32_t)(i - (uint64_t)row * W);
+        out[i] = projection32(x, row_term(row, t.sight_cos), t.sight_sin);
+    }
+}
+
+cudaError_t launch_sight_distances(const SectorTrig &t, uint32_t width, uint32_t height,
+                                   float *out, cudaStream_t s) {
+    k_sight_distances<<<148 * 4, 256, 0, s>>>(t, width, height, out);
+    return cudaGetLastError();
+}
+
+size_t shape_smem_bytes() {
+    return sizeof(ShapeSmem) + (size_t)(kCandidateCap + kWindowCap) * sizeof(unsigned long long);
+}
+
+cudaError_t launch_shape(const ShapeArgs &a, uint32_t n_sectors, cudaStream_t s) {
+    static bool configured = false;
+    const size_t smem = shape_smem_bytes();
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(k_shape, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    uint64_t rank_lo, rank_count;
+    int axes_mode = a.sector_ids_out != nullptr;
+    if (axes_mode) {
+        rank_lo = a.dbg_first;
+        rank_count = a.dbg_count;
+    } else {
+        rank_lo = a.size / 2 - a.band_samples / 2;   // band_of_sight.rs:99-103
+        rank_count = a.band_samples;
+    }
+    k_shape<<<n_sectors, kShapeThreads, smem, s>>>(a, rank_lo, rank_count, axes_mode);
+    return cudaGetLastError();
+}
+
+}  // namespace tvs

@@ -1,0 +1,134 @@
+// tvs_internal.cuh -- shared definitions of the B200 total-viewshed engine.
+//
+// Data layout in HBM (one context):
+//   elevations   f32 [height][width]            uploaded once (main.rs:51-56)
+//   cumulative   f32 [tvs_height][tvs_width]     kernel.rs:254 running sum
+//   total        f32 [tvs_height][tvs_width]     compute.rs:206-214 heatmap total
+//   per sector s (180 slots):
+//     ShapeHeader                                status + step counts + offset bounds
+//     StepTable  float4 {1/d, d, d/R, d*tan1} [step_cap]   sweep constants per step
+//     StepOff    int2   {offset, flags}        [step_cap]   forward DEM-id offset
+//     deltas i32 / distances f32 [band_deltas_size]          band_of_sight.rs output
+//   rings        u32 [total_bands * reserved]   reference ring layout (one sector)
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tvs {
+
+// kernel.rs:13,17,21 and axes.rs:47
+constexpr float kMaxAngle = -2000.0f;
+constexpr float kTanOneRad = 0.0174533f;
+constexpr float kEarthRadiusSquared = 12742000.0f;
+constexpr float kSectorShift = 0.001f;
+constexpr uint32_t kSectorSteps = 180;
+
+// Shape-stage capacities (shared memory of the one-CTA-per-sector kernel).
+constexpr uint32_t kShapeThreads = 1024;
+constexpr uint32_t kCandidateCap = 16384;  // sector-order candidates (u64 each)
+constexpr uint32_t kWindowCap = 8192;      // band_samples (u64 each)
+
+// Step flags.
+constexpr int kStepSlowDivide = 1;  // distance outside the table-division domain
+
+struct SectorTrig {
+    double sight_sin, sight_cos;    // sin/cos(rad(angle + 0.001))         axes.rs:107
+    double sector_sin, sector_cos;  // sin/cos(rad((angle + 0.001) + 90))  axes.rs:127
+};
+
+struct ShapeHeader {
+    int32_t status;        // tvs_status of this sector's shape stage
+    uint32_t n_filled;     // delta-table entries the reference fills
+    uint32_t n_steps;      // steps the sweep evaluates (filled + <= 2 zero-distance)
+    uint32_t n_candidates; // diagnostics: sector-order candidates gathered
+    int64_t min_off;       // min over {0, offsets of evaluated steps}
+    int64_t max_off;
+};
+
+struct ShapeArgs {
+    uint32_t width, height;
+    uint64_t size;
+    uint32_t band_size, band_deltas_size, band_samples;
+    uint32_t first_angle;      // sector of blockIdx.x == 0
+    uint32_t step_cap;         // per-sector stride of the step tables
+    // Extremes of the point-of-view ids (every computable point).
+    int64_t pov_min, pov_max;
+    const SectorTrig *trig;    // [sectors]
+    ShapeHeader *hdr;          // [sectors]
+    float4 *steps;             // [sectors][step_cap]
+    int2 *offs;                // [sectors][step_cap]
+    int32_t *deltas;           // [sectors][band_deltas_size]
+    float *dists;              // [sectors][band_deltas_size]
+    // Optional debug outputs for sector 0 of the launch (tvs_axes):
+    uint32_t *sector_ids_out;  // ranks [dbg_first, dbg_first + dbg_count)
+    uint64_t dbg_first, dbg_count;
+};
+
+struct SweepArgs {
+    const float *elev;
+    uint32_t width;
+    uint32_t tvs_width;
+    uint32_t row_begin, row_end;   // computable rows of this context
+    uint32_t los;                  // max_los_as_points
+    float observer_height;
+    uint32_t n_sectors;
+    uint32_t step_cap;
+    const ShapeHeader *hdr;        // [n_sectors]
+    const float4 *steps;
+    const int2 *offs;
+    float *cumulative;             // f32 [tvs_h * tvs_w]
+    float *total;                  // f32 heatmap total (nullable)
+    double *cumulative64;          // MIXED64/FP64 accumulation (nullable)
+    // Ring output (one sector per launch when non-null).
+    uint32_t *rings;
+    uint32_t reserved;
+    uint64_t half_bands;           // computable_points_count
+    uint4 *spill;                  // {kernel id lo, kernel id hi, slot, value}
+    uint32_t spill_cap;
+    uint32_t *counters;            // [0] spill count [1] overflow bands [2] max ids
+};
+
+struct PlainArgs {
+    const float *elev;
+    uint32_t width, tvs_width, los;
+    uint32_t row_begin, row_end;
+    float observer_height;
+    uint32_t band_deltas_size;
+    const ShapeHeader *hdr;        // one sector
+    const int32_t *deltas;
+    const float *dists;
+    float *sf, *sb;                // per-point band surfaces of the shard
+    uint32_t *rings;
+    uint32_t reserved;
+    uint64_t half_bands;
+    uint4 *spill;
+    uint32_t spill_cap;
+    uint32_t *counters;
+};
+
+// radsort's order-preserving f32 -> u32 key (total order, -0.0 < +0.0).
+__host__ __device__ inline uint32_t f32_radix_key(float f) {
+#ifdef __CUDA_ARCH__
+    uint32_t bits = __float_as_uint(f);
+#else
+    uint32_t bits;
+    __builtin_memcpy(&bits, &f, 4);
+#endif
+    uint32_t mask = (uint32_t)(-(int32_t)(bits >> 31)) | 0x80000000u;
+    return bits ^ mask;
+}
+
+// Host launchers (shape.cu, sweep.cu).
+cudaError_t launch_shape(const ShapeArgs &a, uint32_t n_sectors, cudaStream_t s);
+cudaError_t launch_sight_distances(const SectorTrig &t, uint32_t width, uint32_t height,
+                                   float *out, cudaStream_t s);
+cudaError_t launch_sweep_engine(const SweepArgs &a, int precision, cudaStream_t s);
+cudaError_t launch_sweep_plain(const PlainArgs &a, cudaStream_t s);
+cudaError_t launch_combine(float *cum, float *total, const float *sf, const float *sb,
+                           uint64_t n, cudaStream_t s);
+cudaError_t measure_fp32_issue(double *instructions_per_second);
+cudaError_t launch_selftest_division(uint64_t n, uint64_t seed, unsigned long long *mismatches,
+                                     cudaStream_t s);
+
+}  // namespace tvs
