@@ -33,6 +33,12 @@ METRIC = "LOS samples/s & s per 180-sector TVS, 3601² DEM: mixed vs FP32 on 1 B
 UNIT = "LOS samples/s"
 SECTORS = 180
 FLUSH_BYTES = 256 << 20  # > 126 MB L2
+WORKLOADS = {
+    "precision": "precision form (ridged multifractal, 10% flat 0 m)",
+    "plain_gpu": "plain FP32 GPU form (fBm Hurst 0.75, 15% flat 0 m)",
+    "plain_cpu": "plain CPU-runnable form (fBm Hurst 0.8)",
+    "large": "large single region (2x2 stitched fBm)",
+}
 
 
 def load_package():
@@ -361,9 +367,10 @@ def main():
             "dtype": {"exact32": "f32", "fp64": "f64", "mixed64": "f32+f64"}[args.precision],
             "data": "synthetic",
             "config": {
-                "workload": f"precision form: {cfg['width']}x{cfg['width']} ridged-multifractal DEM "
-                            f"(10% flat 0 m), 30 m cells, LOS {g.max_los_as_points} cells, "
-                            "180 sectors, observer 1.65 m",
+                "workload": WORKLOADS.get(args.config, args.config) +
+                            f": {cfg['width']}x{cfg['width']} DEM, {cfg['scale']:g} m cells, "
+                            f"LOS {g.max_los_as_points} cells, 180 sectors, observer "
+                            f"{cfg['observer_height']} m",
                 "precision": args.precision, "sweep_kernel": args.kernel,
                 "l2": "flushed between steps (256 MiB write); DEM 52 MB is L2-resident within a step",
                 "s_per_tvs": total_ms / args.steps * 1e-3 / 1.0,

@@ -54,6 +54,14 @@ def build(force=False, verbose=False, ptxas_info=False):
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
+    cli_src = PKG / "host" / "tvs_cli.cpp"
+    if force or _stale(CLI, [cli_src, ROOT / "include" / "tvs.h", LIB]):
+        cxx = shutil.which("g++") or "g++"
+        cmd = [cxx, "-O2", "-std=c++17", "-ffp-contract=off", "-I", str(ROOT / "include"),
+               str(cli_src), "-L", str(PKG), "-ltvs_cuda", "-Wl,-rpath,$ORIGIN", "-o", str(CLI)]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
     return LIB
 
 
