@@ -3,7 +3,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -28,6 +30,12 @@ struct tvs_context {
     tvs::ShapeHeader *d_hdr = nullptr;   // [180 + 1]: the last slot serves tvs_axes
     float4 *d_steps = nullptr;
     int2 *d_offs = nullptr;
+    double4 *d_dtab = nullptr;
+    // persistent-sweep work queue
+    uint32_t *d_queue = nullptr;
+    uint32_t *d_done = nullptr;
+    uint32_t done_cap = 0;
+    int32_t *d_error = nullptr;
     int32_t *d_deltas = nullptr;
     float *d_dists = nullptr;
     // ring output (allocated on first use)
@@ -158,8 +166,9 @@ int derive_geometry(const tvs_params *p, tvs_geometry *g, std::string *msg) {
 
 void free_all(tvs_context *c) {
     void *ptrs[] = {c->d_elev, c->d_cum, c->d_total, c->d_cum64, c->d_trig, c->d_hdr,
-                    c->d_steps, c->d_offs, c->d_deltas, c->d_dists, c->d_rings, c->d_spill,
-                    c->d_counters, c->d_sf, c->d_sb};
+                    c->d_steps, c->d_offs, c->d_dtab, c->d_queue, c->d_done, c->d_error,
+                    c->d_deltas, c->d_dists, c->d_rings, c->d_spill, c->d_counters, c->d_sf,
+                    c->d_sb};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -181,6 +190,7 @@ tvs::ShapeArgs shape_args(tvs_context *c, uint32_t first_slot) {
     a.hdr = c->d_hdr + first_slot;
     a.steps = c->d_steps + (uint64_t)first_slot * c->step_cap;
     a.offs = c->d_offs + (uint64_t)first_slot * c->step_cap;
+    a.dtab = c->d_dtab + (uint64_t)first_slot * c->step_cap;
     a.deltas = c->d_deltas + (uint64_t)first_slot * c->g.band_deltas_size;
     a.dists = c->d_dists + (uint64_t)first_slot * c->g.band_deltas_size;
     return a;
@@ -206,6 +216,48 @@ tvs::SweepArgs sweep_args(tvs_context *c, uint32_t first, uint32_t count) {
     a.reserved = c->g.reserved_rings_per_band;
     a.half_bands = c->g.computable_points_count;
     return a;
+}
+
+// Orders, on the GPU, every sequence of constant-table launches on one device:
+// each sequence waits for the previous one (whatever stream it ran on) and
+// becomes the one the next sequence waits for.
+struct DeviceConstLock {
+    static std::mutex &mutex() {
+        static std::mutex m;
+        return m;
+    }
+    static cudaEvent_t &last(int device) {
+        static cudaEvent_t events[64] = {};
+        return events[device & 63];
+    }
+    std::lock_guard<std::mutex> guard;
+    cudaStream_t stream;
+    int device;
+    cudaError_t error = cudaSuccess;
+    DeviceConstLock(int dev, cudaStream_t s) : guard(mutex()), stream(s), device(dev) {
+        cudaEvent_t &ev = last(device);
+        if (!ev) error = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (error == cudaSuccess) error = cudaStreamWaitEvent(stream, ev, 0);
+    }
+    ~DeviceConstLock() {
+        if (error == cudaSuccess) cudaEventRecord(last(device), stream);
+    }
+};
+
+// Sweep implementation for surface-only runs: the persistent work-queue
+// kernel (default), per-sector constant-table launches, or the one-launch
+// shared-memory kernel.  TVS_SWEEP_IMPL=queue|const|smem selects one for
+// comparisons; ring output always uses the shared-memory kernel.
+enum class SweepImpl { Queue, Const, Smem };
+
+SweepImpl sweep_impl() {
+    static SweepImpl v = [] {
+        const char *e = getenv("TVS_SWEEP_IMPL");
+        if (e && !strcmp(e, "const")) return SweepImpl::Const;
+        if (e && !strcmp(e, "smem")) return SweepImpl::Smem;
+        return SweepImpl::Queue;
+    }();
+    return v;
 }
 
 int ensure_rings(tvs_context *c) {
@@ -276,6 +328,51 @@ int enqueue_sweep(tvs_context *c, uint32_t first, uint32_t count, bool rings) {
             TVS_CUDA(c, tvs::launch_combine(c->d_cum + off, c->d_total + off, c->d_sf, c->d_sb,
                                             n, c->stream));
             c->launches += 2;
+        }
+        return TVS_OK;
+    }
+    const uint32_t n_steps =
+        c->g.band_steps_filled + std::min(c->g.band_deltas_size - c->g.band_steps_filled, 2u);
+    const SweepImpl impl = sweep_impl();
+    if (!rings && impl == SweepImpl::Queue) {
+        tvs::QueueArgs q{};
+        q.elev = c->d_elev;
+        q.width = c->g.width;
+        q.tvs_width = c->g.tvs_width;
+        q.los = c->g.max_los_as_points;
+        q.row_begin = c->row_begin;
+        q.row_end = c->row_end;
+        q.observer_height = c->p.observer_height;
+        q.first_sector = first;
+        q.n_sectors = count;
+        q.step_cap = c->step_cap;
+        q.hdr = c->d_hdr;
+        q.steps = c->d_steps;
+        q.offs = c->d_offs;
+        q.dtab = c->d_dtab;
+        q.cumulative = c->d_cum;
+        q.total = c->d_total;
+        q.cumulative64 = c->d_cum64;
+        q.queue = c->d_queue;
+        q.done = c->d_done;
+        q.done_cap = c->done_cap;
+        q.error = c->d_error;
+        q.spin_limit = 1u << 23;  // ~2-4 s of 256 ns sleeps; a real wait is one item (~1 ms)
+        TVS_CUDA(c, tvs::launch_sweep_queue(q, (int)c->p.precision, c->stream));
+        c->launches++;
+        return TVS_OK;
+    }
+    if (!rings && impl == SweepImpl::Const && c->p.precision == TVS_PRECISION_EXACT32 &&
+        n_steps <= tvs::kConstSteps) {
+        // Per-sector launches read the step table from the module's constant
+        // memory, which every context on the device shares: serialise those
+        // launch sequences on the GPU timeline across contexts.
+        DeviceConstLock lock(c->p.device, c->stream);
+        if (lock.error != cudaSuccess) return cuda_fail(c, lock.error, "constant-table lock");
+        for (uint32_t s = first; s < first + count; s++) {
+            tvs::SweepArgs a = sweep_args(c, s, 1);
+            TVS_CUDA(c, tvs::launch_sweep_const(a, (int)c->p.precision, n_steps, c->stream));
+            c->launches++;
         }
         return TVS_OK;
     }
@@ -411,6 +508,7 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
         c->pov_max = (int64_t)((g.tvs_height - 1 + los) * g.width + (g.tvs_width - 1 + los));
     }
     c->step_cap = (g.band_steps_filled + 2 + 3) & ~3u;
+    c->done_cap = tvs::queue_tiles_bound(g.tvs_width, re - rb);
     auto bail = [&](cudaError_t e, const char *what) {
         std::string m = std::string(what) + ": " + cudaGetErrorString(e);
         int code = e == cudaErrorMemoryAllocation ? TVS_ERR_OUT_OF_MEMORY : TVS_ERR_CUDA;
@@ -427,13 +525,17 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
     const uint32_t slots = tvs::kSectorSteps + 1;
     const uint64_t bds = std::max<uint32_t>(g.band_deltas_size, 1);
     struct { void **p; size_t bytes; } allocs[] = {
-        {(void **)&c->d_elev, g.size * sizeof(float)},
+        {(void **)&c->d_elev, (g.size + tvs::kElevationPad) * sizeof(float)},
         {(void **)&c->d_cum, count * sizeof(float)},
         {(void **)&c->d_total, count * sizeof(float)},
         {(void **)&c->d_trig, slots * sizeof(tvs::SectorTrig)},
         {(void **)&c->d_hdr, slots * sizeof(tvs::ShapeHeader)},
         {(void **)&c->d_steps, (size_t)slots * c->step_cap * sizeof(float4)},
         {(void **)&c->d_offs, (size_t)slots * c->step_cap * sizeof(int2)},
+        {(void **)&c->d_dtab, (size_t)slots * c->step_cap * sizeof(double4)},
+        {(void **)&c->d_queue, sizeof(uint32_t)},
+        {(void **)&c->d_done, (size_t)std::max<uint32_t>(c->done_cap, 1) * sizeof(uint32_t)},
+        {(void **)&c->d_error, sizeof(int32_t)},
         {(void **)&c->d_deltas, (size_t)slots * bds * sizeof(int32_t)},
         {(void **)&c->d_dists, (size_t)slots * bds * sizeof(float)},
     };
@@ -460,7 +562,10 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
     if ((e = cudaMemcpy(c->d_elev, elevations, g.size * sizeof(float), cudaMemcpyHostToDevice)) !=
         cudaSuccess)
         return bail(e, "cudaMemcpy elevations");
+    if ((e = cudaMemset(c->d_elev + g.size, 0, tvs::kElevationPad * sizeof(float))) != cudaSuccess)
+        return bail(e, "cudaMemset elevation padding");
     if ((e = cudaMemset(c->d_hdr, 0, slots * sizeof(tvs::ShapeHeader))) != cudaSuccess ||
+        (e = cudaMemset(c->d_error, 0, sizeof(int32_t))) != cudaSuccess ||
         (e = cudaMemset(c->d_cum, 0, count * sizeof(float))) != cudaSuccess ||
         (e = cudaMemset(c->d_total, 0, count * sizeof(float))) != cudaSuccess)
         return bail(e, "cudaMemset");
@@ -664,6 +769,14 @@ int tvs_device_finish(tvs_context *ctx) {
         s = e - 1;
     }
     for (bool &p : ctx->pending) p = false;
+    int32_t err = 0;
+    TVS_CUDA(ctx, cudaMemcpy(&err, ctx->d_error, sizeof err, cudaMemcpyDeviceToHost));
+    if (err != 0) {
+        TVS_CUDA(ctx, cudaMemset(ctx->d_error, 0, sizeof err));
+        if (rc == TVS_OK)
+            rc = fail(ctx, err, "sweep work queue: a tile's dependency wait gave up "
+                                "(iteration limit); results of this run are incomplete");
+    }
     return rc;
 }
 

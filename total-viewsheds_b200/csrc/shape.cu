@@ -256,6 +256,7 @@ k_shape(ShapeArgs a, uint64_t rank_lo, uint64_t rank_count, int axes_mode) {
 
     // 5. Step tables: steps past n_filled repeat the last offset with d = 0.
     long long mn = 0, mx = 0;
+    uint32_t first_slow = n_steps;
     float4 *gsteps = a.steps + (uint64_t)sector * a.step_cap;
     int2 *goffs = a.offs + (uint64_t)sector * a.step_cap;
     for (uint32_t i = threadIdx.x; i < n_steps; i += blockDim.x) {
@@ -269,9 +270,22 @@ k_shape(ShapeArgs a, uint64_t rank_lo, uint64_t rank_count, int axes_mode) {
         int flags = (d >= 0x1p-20f && d <= 0x1p20f) ? 0 : kStepSlowDivide;
         gsteps[i] = st;
         goffs[i] = make_int2((int32_t)off, flags);
+        // FP64 sweep tables: the same distance in double (kernel.rs:175,216)
+        const double dd = (double)d;
+        a.dtab[(uint64_t)sector * a.step_cap + i] =
+            make_double4(__drcp_rn(dd), __ddiv_rn(dd, 12742000.0), __dmul_rn(dd, 0.0174533), 0.0);
         mn = min(mn, off);
         mx = max(mx, off);
+        if (flags) first_slow = min(first_slow, i);
     }
+    __syncthreads();
+    sm.scan[threadIdx.x] = first_slow;
+    __syncthreads();
+    for (uint32_t o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sm.scan[threadIdx.x] = min(sm.scan[threadIdx.x], sm.scan[threadIdx.x + o]);
+        __syncthreads();
+    }
+    const uint32_t n_fast = (uint32_t)sm.scan[0];
     __syncthreads();
     // block min / max through the scan scratch
     sm.scan[threadIdx.x] = mn;
@@ -301,6 +315,7 @@ k_shape(ShapeArgs a, uint64_t rank_lo, uint64_t rank_count, int axes_mode) {
         hdr->n_candidates = n_cand;
         hdr->min_off = min_off;
         hdr->max_off = max_off;
+        hdr->n_fast = n_fast;
     }
 }
 

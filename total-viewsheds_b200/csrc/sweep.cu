@@ -38,6 +38,9 @@
 //
 // All adds, subtracts and multiplies use the _rn intrinsics so nvcc cannot
 // contract them into FMAs; the results are bit-identical to the reference.
+#include <cstdio>
+#include <cstdlib>
+
 #include "tvs.h"
 #include "tvs_internal.cuh"
 
@@ -162,6 +165,101 @@ k_sweep_exact32(SweepArgs a) {
     if (active) {
         a.cumulative[tvs] = cum;
         if (a.total) a.total[tvs] = tot;
+    }
+}
+
+// Per-sector launch with the sector's step table in constant memory.  A thread
+// sweeps kPx x kPy points of view, both directions: columns tx + 32*px share
+// one address per step (the +128*px bytes are load immediates) and rows
+// ty + 8*py share the table operands, so each step feeds 2*kPx*kPy independent
+// chains.  Steps [0, n_fast) take the table division with no per-step test;
+// the rest (the zero-distance tail) test the distance.  Lanes past the
+// computable grid sweep a clamped row / an unused column and are discarded;
+// the elevation buffer is padded so their loads stay inside the allocation.
+__constant__ ShapeHeader c_hdr;
+__constant__ float4 c_steps[kConstSteps];
+__constant__ int2 c_offs[kConstSteps];
+
+template <int kPx, int kPy>
+__global__ void __launch_bounds__(kTileX * kTileY)
+k_sweep_exact32_const(SweepArgs a) {
+    if (c_hdr.status != TVS_OK) return;
+    const uint32_t n = c_hdr.n_steps, n_fast = c_hdr.n_fast;
+    const uint32_t tx0 = blockIdx.x * (kTileX * kPx) + threadIdx.x;
+    const uint32_t ty0 = a.row_begin + blockIdx.y * (kTileY * kPy) + threadIdx.y;
+    const float *ep[kPy];
+    float hp[kPy][kPx], mf[kPy][kPx], mb[kPy][kPx], sf[kPy][kPx], sb[kPy][kPx];
+#pragma unroll
+    for (int py = 0; py < kPy; py++) {
+        const uint32_t ty = min(ty0 + py * kTileY, a.row_end - 1);
+        ep[py] = a.elev + (int64_t)(ty + a.los) * a.width + tx0 + a.los;
+#pragma unroll
+        for (int px = 0; px < kPx; px++) {
+            hp[py][px] = __fadd_rn(__ldg(ep[py] + kTileX * px), a.observer_height);  // kernel.rs:134
+            mf[py][px] = mb[py][px] = kMaxAngle;
+            sf[py][px] = sb[py][px] = 0.0f;
+        }
+    }
+    uint32_t i = 0;
+#pragma unroll 2
+    for (; i < n_fast; i++) {
+        const float4 t = c_steps[i];
+        const int32_t o = c_offs[i].x;
+#pragma unroll
+        for (int py = 0; py < kPy; py++) {
+            const float *pf = ep[py] + o;
+            const float *pb = ep[py] - o;
+#pragma unroll
+            for (int px = 0; px < kPx; px++) {
+                const float af = __fsub_rn(
+                    table_divide(__fsub_rn(__ldg(pf + kTileX * px), hp[py][px]), t.x, t.y), t.z);
+                const float ab = __fsub_rn(
+                    table_divide(__fsub_rn(__ldg(pb + kTileX * px), hp[py][px]), t.x, t.y), t.z);
+                if (af > mf[py][px]) sf[py][px] = __fadd_rn(sf[py][px], t.w);
+                if (ab > mb[py][px]) sb[py][px] = __fadd_rn(sb[py][px], t.w);
+                mf[py][px] = fmaxf(af, mf[py][px]);
+                mb[py][px] = fmaxf(ab, mb[py][px]);
+            }
+        }
+    }
+    for (; i < n; i++) {
+        const float4 t = c_steps[i];
+        const int2 o = c_offs[i];
+#pragma unroll
+        for (int py = 0; py < kPy; py++) {
+#pragma unroll
+            for (int px = 0; px < kPx; px++) {
+                const float ef = __fsub_rn(__ldg(ep[py] + o.x + kTileX * px), hp[py][px]);
+                const float eb = __fsub_rn(__ldg(ep[py] - o.x + kTileX * px), hp[py][px]);
+                float qf, qb;
+                if (o.y == 0) {
+                    qf = table_divide(ef, t.x, t.y);
+                    qb = table_divide(eb, t.x, t.y);
+                } else {
+                    qf = __fdiv_rn(ef, t.y);
+                    qb = __fdiv_rn(eb, t.y);
+                }
+                const float af = __fsub_rn(qf, t.z), ab = __fsub_rn(qb, t.z);
+                if (af > mf[py][px]) sf[py][px] = __fadd_rn(sf[py][px], t.w);
+                if (ab > mb[py][px]) sb[py][px] = __fadd_rn(sb[py][px], t.w);
+                mf[py][px] = fmaxf(af, mf[py][px]);
+                mb[py][px] = fmaxf(ab, mb[py][px]);
+            }
+        }
+    }
+#pragma unroll
+    for (int py = 0; py < kPy; py++) {
+        const uint32_t ty = ty0 + py * kTileY;
+        if (ty >= a.row_end) continue;
+#pragma unroll
+        for (int px = 0; px < kPx; px++) {
+            const uint32_t tx = tx0 + kTileX * px;
+            if (tx >= a.tvs_width) continue;
+            const uint64_t tvs = (uint64_t)ty * a.tvs_width + tx;
+            const float cum = __fadd_rn(__fadd_rn(a.cumulative[tvs], sf[py][px]), sb[py][px]);
+            a.cumulative[tvs] = cum;                                   // kernel.rs:254
+            if (a.total) a.total[tvs] = __fadd_rn(a.total[tvs], cum);  // compute.rs:206-214
+        }
     }
 }
 
@@ -304,6 +402,10 @@ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
     return x ^ (x >> 31);
 }
 
+__device__ __forceinline__ float h_like(uint64_t r) {
+    return (float)((int32_t)((r >> 20) & 0xFFFFF) - 0x40000) * 0.03125f;
+}
+
 // Random (numerator, distance) pairs: distances log-uniform over the table
 // domain [2^-20, 2^20]; numerators either log-uniform over +-[2^-60, 2^60] or
 // elevation-like differences (f32 heights minus an observer height).
@@ -329,6 +431,17 @@ __global__ void k_selftest_division(uint64_t n, uint64_t seed, unsigned long lon
         float got = table_divide(e, y, d);
         float want = __fdiv_rn(e, d);
         if (__float_as_uint(got) != __float_as_uint(want)) local++;
+        // double: numerators with 53 random mantissa bits, the same f32 distances
+        uint64_t r2 = splitmix64(r1);
+        uint64_t eexp = 1023u - 60u + (r2 % 121u);
+        double e64 = __longlong_as_double((long long)(((r2 >> 63) << 63) | (eexp << 52) |
+                                                      (splitmix64(r2) >> 12)));
+        if (r1 & 2) e64 = __dsub_rn((double)h_like(r2), __dadd_rn((double)h_like(r1), 1.65));
+        double d64 = (double)d;
+        double q = __dmul_rn(e64, __drcp_rn(d64));
+        double r = __fma_rn(-d64, q, e64);
+        double got64 = __fma_rn(r, __drcp_rn(d64), q);
+        if (__double_as_longlong(got64) != __double_as_longlong(__ddiv_rn(e64, d64))) local++;
     }
     if (local) atomicAdd(mismatches, local);
 }
@@ -397,6 +510,54 @@ cudaError_t launch_sweep_engine(const SweepArgs &a, int precision, cudaStream_t 
                                          (int)smem);
     if (e != cudaSuccess) return e;
     fn<<<grid, block, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+// Points of view per thread of the constant-table sweep: columns x rows.
+// TVS_SWEEP_SHAPE ("4x1", "2x2", "2x1", "1x2", "1x1", "8x1") overrides the default
+// for tuning runs.
+struct PovShape { int px, py; };
+
+PovShape const_shape() {
+    static PovShape v = [] {
+        const char *e = getenv("TVS_SWEEP_SHAPE");
+        PovShape d{4, 1};
+        if (!e) return d;
+        int x = 0, y = 0;
+        if (sscanf(e, "%dx%d", &x, &y) != 2) return d;
+        const PovShape ok[] = {{1, 1}, {2, 1}, {1, 2}, {2, 2}, {4, 1}, {8, 1}, {4, 2}};
+        for (const PovShape &k : ok)
+            if (k.px == x && k.py == y) return k;
+        return d;
+    }();
+    return v;
+}
+
+cudaError_t launch_sweep_const(const SweepArgs &a, int precision, uint32_t n_steps,
+                               cudaStream_t s) {
+    if (precision != TVS_PRECISION_EXACT32 || a.rings || a.n_sectors != 1 || n_steps > kConstSteps)
+        return cudaErrorInvalidValue;
+    const uint32_t rows = a.row_end - a.row_begin;
+    if (rows == 0 || a.tvs_width == 0) return cudaSuccess;
+    cudaError_t e = cudaMemcpyToSymbolAsync(c_hdr, a.hdr, sizeof(ShapeHeader), 0,
+                                            cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess && n_steps)
+        e = cudaMemcpyToSymbolAsync(c_steps, a.steps, n_steps * sizeof(float4), 0,
+                                    cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess && n_steps)
+        e = cudaMemcpyToSymbolAsync(c_offs, a.offs, n_steps * sizeof(int2), 0,
+                                    cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return e;
+    const PovShape sh = const_shape();
+    dim3 block(kTileX, kTileY);
+    dim3 grid((a.tvs_width + kTileX * sh.px - 1) / (kTileX * sh.px),
+              (rows + kTileY * sh.py - 1) / (kTileY * sh.py));
+#define TVS_CONST_CASE(X, Y) \
+    if (sh.px == X && sh.py == Y) k_sweep_exact32_const<X, Y><<<grid, block, 0, s>>>(a); else
+    TVS_CONST_CASE(1, 1) TVS_CONST_CASE(2, 1) TVS_CONST_CASE(1, 2) TVS_CONST_CASE(2, 2)
+    TVS_CONST_CASE(8, 1) TVS_CONST_CASE(4, 2)
+    k_sweep_exact32_const<4, 1><<<grid, block, 0, s>>>(a);
+#undef TVS_CONST_CASE
     return cudaGetLastError();
 }
 

@@ -1,0 +1,334 @@
+// sweep_queue.cu -- persistent band-of-sight sweep over a (sector, tile) work queue.
+//
+// The arithmetic is the reference kernel's (kernel.rs:153-254), as in sweep.cu;
+// this file changes how the work is scheduled so that no wave of CTAs runs
+// half empty:
+//
+//  * The grid is exactly the resident capacity of the GPU (occupancy x SMs).
+//    Each CTA repeatedly takes the next work item from a global counter.
+//  * Items are (sector, tile) pairs in sector-major order, so a CTA mostly
+//    stays on one sector and re-stages its step tables in shared memory only
+//    when the sector changes.
+//  * A tile's sectors must be applied in order (the reference adds sector
+//    surfaces to each point's cumulative sum sector by sector, f32).  Each
+//    tile has a counter of completed sectors; the item (s, T) waits until the
+//    counter of T reaches s.  (s-1, T) was dequeued earlier by a CTA that is
+//    running, so the wait always ends; it is bounded anyway (spin limit ->
+//    TVS_ERR_TIMEOUT in the error word, the item is skipped, the run fails).
+//  * A thread sweeps kPx x kPy points of view: columns 32 apart share one
+//    address per step (load immediates), rows 8 apart share the table
+//    operands.  Forward and backward bands of a point of view run in the same
+//    loop; cum = (cum + forward) + backward keeps the reference's order.
+//  * Steps [0, n_fast) use the table division (Markstein, see sweep.cu) with
+//    no per-step test; the zero-distance tail uses IEEE division.
+//
+// Precision kPrec: TVS_PRECISION_EXACT32 (reference f32, bit-exact) or
+// TVS_PRECISION_FP64 (the same control flow in double: angles, maximum and
+// surfaces; table division in double from y = RN64(1/d)).
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <type_traits>
+
+#include "tvs.h"
+#include "tvs_internal.cuh"
+
+namespace tvs {
+namespace {
+
+constexpr int kTileX = 32;
+constexpr int kTileY = 8;
+constexpr int kThreads = kTileX * kTileY;
+
+__device__ __forceinline__ float div_table32(float e, float y, float d) {
+    const float q = __fmul_rn(e, y);
+    const float r = __fmaf_rn(-d, q, e);
+    return __fmaf_rn(r, y, q);
+}
+
+__device__ __forceinline__ double div_table64(double e, double y, double d) {
+    const double q = __dmul_rn(e, y);
+    const double r = __fma_rn(-d, q, e);
+    return __fma_rn(r, y, q);
+}
+
+struct QueueCtl {
+    uint32_t item;
+    int32_t sector_status;  // the staged sector's shape status
+    int32_t wait_status;    // this item's dependency wait
+    uint32_t n_steps;
+    uint32_t n_fast;
+    uint32_t pad[3];
+};
+
+// Per-point state of one direction.
+template <int kPrec> struct Chain;
+template <> struct Chain<TVS_PRECISION_EXACT32> {
+    float m, s;
+    __device__ void init() { m = kMaxAngle; s = 0.0f; }
+};
+template <> struct Chain<TVS_PRECISION_FP64> {
+    double m, s;
+    __device__ void init() { m = -2000.0; s = 0.0; }
+};
+
+template <int kPrec, bool kFast>
+__device__ __forceinline__ void step_f32(Chain<kPrec> &c, float h, float hp, const float4 &t,
+                                         int slow) {
+    const float e = __fsub_rn(h, hp);
+    float q;
+    if (kFast || !slow) q = div_table32(e, t.x, t.y);
+    else q = __fdiv_rn(e, t.y);
+    const float a = __fsub_rn(q, t.z);
+    if (a > c.m) c.s = __fadd_rn(c.s, t.w);
+    c.m = fmaxf(a, c.m);  // f32::max: NaN yields the other operand
+}
+
+template <int kPrec, bool kFast>
+__device__ __forceinline__ void step_f64(Chain<kPrec> &c, float h, double hp, float d,
+                                         const double4 &t, int slow) {
+    const double e = __dsub_rn((double)h, hp);
+    double q;
+    if (kFast || !slow) q = div_table64(e, t.x, (double)d);
+    else q = __ddiv_rn(e, (double)d);
+    const double a = __dsub_rn(q, t.y);
+    if (a > c.m) c.s = __dadd_rn(c.s, t.z);
+    c.m = fmax(a, c.m);
+}
+
+template <int kPrec, int kPx, int kPy>
+__global__ void __launch_bounds__(kThreads)
+k_sweep_queue(QueueArgs a) {
+    constexpr bool kF64 = kPrec == TVS_PRECISION_FP64;
+    extern __shared__ __align__(16) unsigned char smem[];
+    QueueCtl &ctl = *reinterpret_cast<QueueCtl *>(smem);
+    float4 *s_steps = reinterpret_cast<float4 *>(smem + sizeof(QueueCtl));
+    int2 *s_offs = reinterpret_cast<int2 *>(s_steps + a.step_cap);
+    double4 *s_dtab = reinterpret_cast<double4 *>(s_offs + a.step_cap);  // FP64 only
+    const uint32_t tid = threadIdx.y * kTileX + threadIdx.x;
+    const uint32_t n_tiles = a.tiles_x * a.tiles_y;
+    const uint32_t n_items = n_tiles * a.n_sectors;
+    uint32_t cur = 0xFFFFFFFFu;
+
+    for (;;) {
+        if (tid == 0) ctl.item = atomicAdd(a.queue, 1u);
+        __syncthreads();
+        const uint32_t item = ctl.item;
+        if (item >= n_items) break;
+        const uint32_t s = item / n_tiles, tile = item - s * n_tiles;
+        if (s != cur) {  // stage this sector's tables
+            const uint32_t slot = a.first_sector + s;
+            const ShapeHeader *h = a.hdr + slot;
+            const uint32_t n = h->n_steps;
+            const float4 *gs = a.steps + (uint64_t)slot * a.step_cap;
+            const int2 *go = a.offs + (uint64_t)slot * a.step_cap;
+            for (uint32_t i = tid; i < n; i += kThreads) {
+                s_steps[i] = gs[i];
+                s_offs[i] = go[i];
+                if (kF64) s_dtab[i] = a.dtab[(uint64_t)slot * a.step_cap + i];
+            }
+            if (tid == 0) {
+                ctl.sector_status = h->status;
+                ctl.n_steps = n;
+                ctl.n_fast = h->n_fast;
+            }
+            cur = s;
+        }
+        // This tile's previous sector must be complete (bounded wait).
+        if (tid == 0) {
+            ctl.wait_status = TVS_OK;
+            if (s > 0) {
+                const volatile uint32_t *d = a.done + tile;
+                const volatile int32_t *err = a.error;
+                uint32_t spins = 0;
+                while (*d < s) {
+                    // give up at the limit, or at once when another wait already did
+                    if (++spins > a.spin_limit || *err != 0) {
+                        atomicExch(a.error, (int32_t)TVS_ERR_TIMEOUT);
+                        ctl.wait_status = TVS_ERR_TIMEOUT;
+                        break;
+                    }
+                    __nanosleep(256);
+                }
+                __threadfence();
+            }
+        }
+        __syncthreads();
+        const bool run = ctl.sector_status == TVS_OK && ctl.wait_status == TVS_OK;
+        const uint32_t n = ctl.n_steps, n_fast = ctl.n_fast;
+        const uint32_t bx = tile % a.tiles_x, by = tile / a.tiles_x;
+        const uint32_t tx0 = bx * (kTileX * kPx) + threadIdx.x;
+        const uint32_t ty0 = a.row_begin + by * (kTileY * kPy) + threadIdx.y;
+        if (run) {
+            const float *ep[kPy];
+            using HP = typename std::conditional<kF64, double, float>::type;
+            HP hp[kPy][kPx];
+            Chain<kPrec> cf[kPy][kPx], cb[kPy][kPx];
+#pragma unroll
+            for (int py = 0; py < kPy; py++) {
+                // rows past the grid are clamped, columns past it read padding;
+                // both are discarded
+                const uint32_t ty = min(ty0 + py * kTileY, a.row_end - 1);
+                ep[py] = a.elev + (int64_t)(ty + a.los) * a.width + tx0 + a.los;
+#pragma unroll
+                for (int px = 0; px < kPx; px++) {
+                    const float h0 = __ldg(ep[py] + kTileX * px);
+                    if (kF64) hp[py][px] = (HP)__dadd_rn((double)h0, (double)a.observer_height);
+                    else hp[py][px] = (HP)__fadd_rn(h0, a.observer_height);  // kernel.rs:134
+                    cf[py][px].init();
+                    cb[py][px].init();
+                }
+            }
+            uint32_t i = 0;
+#pragma unroll 2
+            for (; i < n_fast; i++) {
+                const float4 t = s_steps[i];
+                const int32_t o = s_offs[i].x;
+                double4 dt;
+                if (kF64) dt = s_dtab[i];
+#pragma unroll
+                for (int py = 0; py < kPy; py++) {
+                    const float *pf = ep[py] + o;
+                    const float *pb = ep[py] - o;
+#pragma unroll
+                    for (int px = 0; px < kPx; px++) {
+                        const float hf = __ldg(pf + kTileX * px), hb = __ldg(pb + kTileX * px);
+                        if constexpr (kF64) {
+                            step_f64<kPrec, true>(cf[py][px], hf, hp[py][px], t.y, dt, 0);
+                            step_f64<kPrec, true>(cb[py][px], hb, hp[py][px], t.y, dt, 0);
+                        } else {
+                            step_f32<kPrec, true>(cf[py][px], hf, hp[py][px], t, 0);
+                            step_f32<kPrec, true>(cb[py][px], hb, hp[py][px], t, 0);
+                        }
+                    }
+                }
+            }
+            for (; i < n; i++) {
+                const float4 t = s_steps[i];
+                const int2 o = s_offs[i];
+                double4 dt;
+                if (kF64) dt = s_dtab[i];
+#pragma unroll
+                for (int py = 0; py < kPy; py++) {
+#pragma unroll
+                    for (int px = 0; px < kPx; px++) {
+                        const float hf = __ldg(ep[py] + o.x + kTileX * px);
+                        const float hb = __ldg(ep[py] - o.x + kTileX * px);
+                        if constexpr (kF64) {
+                            step_f64<kPrec, false>(cf[py][px], hf, hp[py][px], t.y, dt, o.y);
+                            step_f64<kPrec, false>(cb[py][px], hb, hp[py][px], t.y, dt, o.y);
+                        } else {
+                            step_f32<kPrec, false>(cf[py][px], hf, hp[py][px], t, o.y);
+                            step_f32<kPrec, false>(cb[py][px], hb, hp[py][px], t, o.y);
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int py = 0; py < kPy; py++) {
+                const uint32_t ty = ty0 + py * kTileY;
+                if (ty >= a.row_end) continue;
+#pragma unroll
+                for (int px = 0; px < kPx; px++) {
+                    const uint32_t tx = tx0 + kTileX * px;
+                    if (tx >= a.tvs_width) continue;
+                    const uint64_t p = (uint64_t)ty * a.tvs_width + tx;
+                    // surfaces are read and written in L2 (another SM wrote the
+                    // previous sector's values)
+                    if constexpr (kF64) {
+                        const double cum =
+                            __dadd_rn(__dadd_rn(__ldcg(a.cumulative64 + p), cf[py][px].s), cb[py][px].s);
+                        __stcg(a.cumulative64 + p, cum);
+                        const float c32 = __double2float_rn(cum);
+                        __stcg(a.cumulative + p, c32);
+                        if (a.total) __stcg(a.total + p, __fadd_rn(__ldcg(a.total + p), c32));
+                    } else {
+                        const float cum =
+                            __fadd_rn(__fadd_rn(__ldcg(a.cumulative + p), cf[py][px].s), cb[py][px].s);
+                        __stcg(a.cumulative + p, cum);                                  // kernel.rs:254
+                        if (a.total) __stcg(a.total + p, __fadd_rn(__ldcg(a.total + p), cum));  // compute.rs:206-214
+                    }
+                }
+            }
+        }
+        __threadfence();   // this thread's surface writes before the tile's counter
+        __syncthreads();
+        if (tid == 0) atomicAdd(a.done + tile, 1u);
+    }
+}
+
+struct PovShape { int px, py; };
+
+PovShape queue_shape() {
+    static PovShape v = [] {
+        const char *e = getenv("TVS_SWEEP_SHAPE");
+        PovShape d{4, 1};
+        if (!e) return d;
+        int x = 0, y = 0;
+        if (sscanf(e, "%dx%d", &x, &y) != 2) return d;
+        const PovShape ok[] = {{1, 1}, {2, 1}, {4, 1}, {2, 2}, {8, 1}};
+        for (const PovShape &k : ok)
+            if (k.px == x && k.py == y) return k;
+        return d;
+    }();
+    return v;
+}
+
+template <int kPrec, int kPx, int kPy>
+cudaError_t launch_queue_t(const QueueArgs &a0, size_t smem, cudaStream_t s) {
+    auto fn = k_sweep_queue<kPrec, kPx, kPy>;
+    static int blocks_per_sm = -1;
+    static size_t configured_smem = 0;
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    if (blocks_per_sm < 0 || configured_smem != smem) {
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, fn, kThreads, smem);
+        if (e != cudaSuccess) return e;
+        if (blocks_per_sm < 1) blocks_per_sm = 1;
+        configured_smem = smem;
+    }
+    QueueArgs a = a0;
+    const uint32_t rows = a.row_end - a.row_begin;
+    a.tiles_x = (a.tvs_width + kTileX * kPx - 1) / (kTileX * kPx);
+    a.tiles_y = (rows + kTileY * kPy - 1) / (kTileY * kPy);
+    const uint64_t tiles = (uint64_t)a.tiles_x * a.tiles_y;
+    if (tiles > a.done_cap) return cudaErrorInvalidValue;
+    e = cudaMemsetAsync(a.queue, 0, sizeof(uint32_t), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(a.done, 0, tiles * sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    const uint64_t items = tiles * a.n_sectors;
+    const uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)blocks_per_sm * sms, items);
+    fn<<<grid, dim3(kTileX, kTileY), smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+uint32_t queue_tiles_bound(uint32_t tvs_width, uint32_t rows) {
+    // the smallest tile (32 x 8 points) bounds the tile count of every shape
+    return ((tvs_width + kTileX - 1) / kTileX) * ((rows + kTileY - 1) / kTileY);
+}
+
+cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, cudaStream_t s) {
+    const uint32_t rows = a.row_end - a.row_begin;
+    if (rows == 0 || a.tvs_width == 0 || a.n_sectors == 0) return cudaSuccess;
+    const bool f64 = precision == TVS_PRECISION_FP64;
+    if (!f64 && precision != TVS_PRECISION_EXACT32) return cudaErrorInvalidValue;
+    const size_t smem = 32 + (size_t)a.step_cap * (sizeof(float4) + sizeof(int2) +
+                                                    (f64 ? sizeof(double4) : 0));
+    const PovShape sh = queue_shape();
+#define TVS_Q(X, Y)                                                                    \
+    if (sh.px == X && sh.py == Y)                                                      \
+        return f64 ? launch_queue_t<TVS_PRECISION_FP64, X, Y>(a, smem, s)              \
+                   : launch_queue_t<TVS_PRECISION_EXACT32, X, Y>(a, smem, s);
+    TVS_Q(1, 1) TVS_Q(2, 1) TVS_Q(2, 2) TVS_Q(8, 1)
+#undef TVS_Q
+    return f64 ? launch_queue_t<TVS_PRECISION_FP64, 4, 1>(a, smem, s)
+               : launch_queue_t<TVS_PRECISION_EXACT32, 4, 1>(a, smem, s);
+}
+
+}  // namespace tvs

@@ -44,7 +44,19 @@ struct ShapeHeader {
     uint32_t n_candidates; // diagnostics: sector-order candidates gathered
     int64_t min_off;       // min over {0, offsets of evaluated steps}
     int64_t max_off;
+    uint32_t n_fast;       // steps before the first kStepSlowDivide step
+    uint32_t pad;
 };
+
+// Per-sector sweep launches read their step table from constant memory, so
+// every table value is a warp-uniform operand (no shared-memory loads, no
+// per-lane table addressing).  2560 steps cover band_steps_filled + 2 for a
+// line of sight of up to ~4360 cells.
+constexpr uint32_t kConstSteps = 2560;
+// Zero floats after the elevations: a constant-table sweep thread covers up to
+// 8 columns 32 apart, so lanes past the computable grid read at most
+// 32*8 + 32 floats beyond the last point of view's band (discarded results).
+constexpr uint32_t kElevationPad = 32 * 8 + 64;
 
 struct ShapeArgs {
     uint32_t width, height;
@@ -58,6 +70,7 @@ struct ShapeArgs {
     ShapeHeader *hdr;          // [sectors]
     float4 *steps;             // [sectors][step_cap]
     int2 *offs;                // [sectors][step_cap]
+    double4 *dtab;             // [sectors][step_cap] FP64 {1/d, d/R, d*tan1, 0}
     int32_t *deltas;           // [sectors][band_deltas_size]
     float *dists;              // [sectors][band_deltas_size]
     // Optional debug outputs for sector 0 of the launch (tvs_axes):
@@ -87,6 +100,29 @@ struct SweepArgs {
     uint4 *spill;                  // {kernel id lo, kernel id hi, slot, value}
     uint32_t spill_cap;
     uint32_t *counters;            // [0] spill count [1] overflow bands [2] max ids
+};
+
+// Persistent sweep over a (sector, tile) work queue (sweep_queue.cu).
+struct QueueArgs {
+    const float *elev;
+    uint32_t width, tvs_width, los;
+    uint32_t row_begin, row_end;
+    float observer_height;
+    uint32_t first_sector, n_sectors;  // absolute sector slots
+    uint32_t step_cap;
+    const ShapeHeader *hdr;            // per-slot arrays (absolute slot index)
+    const float4 *steps;
+    const int2 *offs;
+    const double4 *dtab;               // FP64 tables {1/d, d/R, d*tan1, 0} (double)
+    float *cumulative;
+    float *total;                      // nullable
+    double *cumulative64;              // FP64 only
+    uint32_t tiles_x, tiles_y;         // set by the launcher
+    uint32_t *queue;                   // [1] next work item
+    uint32_t *done;                    // [done_cap] sectors completed per tile
+    uint32_t done_cap;
+    int32_t *error;                    // TVS_ERR_TIMEOUT when a wait gives up
+    uint32_t spin_limit;
 };
 
 struct PlainArgs {
@@ -124,7 +160,13 @@ cudaError_t launch_shape(const ShapeArgs &a, uint32_t n_sectors, cudaStream_t s)
 cudaError_t launch_sight_distances(const SectorTrig &t, uint32_t width, uint32_t height,
                                    float *out, cudaStream_t s);
 cudaError_t launch_sweep_engine(const SweepArgs &a, int precision, cudaStream_t s);
+// One sector per launch with the step table staged in constant memory
+// (hdr/steps/offs point at that sector's tables; a.n_sectors must be 1).
+cudaError_t launch_sweep_const(const SweepArgs &a, int precision, uint32_t n_steps,
+                               cudaStream_t s);
 cudaError_t launch_sweep_plain(const PlainArgs &a, cudaStream_t s);
+cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, cudaStream_t s);
+uint32_t queue_tiles_bound(uint32_t tvs_width, uint32_t rows);
 cudaError_t launch_combine(float *cum, float *total, const float *sf, const float *sb,
                            uint64_t n, cudaStream_t s);
 cudaError_t measure_fp32_issue(double *instructions_per_second);
