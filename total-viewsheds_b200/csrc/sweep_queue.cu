@@ -52,6 +52,45 @@ __device__ __forceinline__ double div_table64(double e, double y, double d) {
     return __fma_rn(r, y, q);
 }
 
+// Packed FP32 pairs (sm_100 f32x2): each element is rounded exactly as the
+// scalar operation, so a (forward, backward) pair goes through one instruction.
+typedef unsigned long long f32x2;
+
+__device__ __forceinline__ f32x2 pk(float lo, float hi) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void upk(f32x2 v, float &lo, float &hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+    f32x2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+    f32x2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+// 1.0f when a > b, else 0.0f (false for NaN operands, like the reference's `>`)
+__device__ __forceinline__ float gt01(float a, float b) {
+    float r;
+    asm("set.gt.f32.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
+
+// One packed table entry: {y, y}, {-d, -d}, {d/R, d/R}, {d*tan1, d*tan1}.
+struct PackedStep {
+    f32x2 y, nd, c, w;
+};
+
 struct QueueCtl {
     uint32_t item;
     int32_t sector_status;  // the staged sector's shape status
@@ -105,6 +144,7 @@ k_sweep_queue(QueueArgs a) {
     float4 *s_steps = reinterpret_cast<float4 *>(smem + sizeof(QueueCtl));
     int2 *s_offs = reinterpret_cast<int2 *>(s_steps + a.step_cap);
     double4 *s_dtab = reinterpret_cast<double4 *>(s_offs + a.step_cap);  // FP64 only
+    PackedStep *s_pk = reinterpret_cast<PackedStep *>(s_offs + a.step_cap);  // EXACT32 only
     const uint32_t tid = threadIdx.y * kTileX + threadIdx.x;
     const uint32_t n_tiles = a.tiles_x * a.tiles_y;
     const uint32_t n_items = n_tiles * a.n_sectors;
@@ -123,9 +163,19 @@ k_sweep_queue(QueueArgs a) {
             const float4 *gs = a.steps + (uint64_t)slot * a.step_cap;
             const int2 *go = a.offs + (uint64_t)slot * a.step_cap;
             for (uint32_t i = tid; i < n; i += kThreads) {
-                s_steps[i] = gs[i];
+                const float4 t = gs[i];
+                s_steps[i] = t;
                 s_offs[i] = go[i];
-                if (kF64) s_dtab[i] = a.dtab[(uint64_t)slot * a.step_cap + i];
+                if (kF64) {
+                    s_dtab[i] = a.dtab[(uint64_t)slot * a.step_cap + i];
+                } else {
+                    PackedStep p;
+                    p.y = pk(t.x, t.x);
+                    p.nd = pk(-t.y, -t.y);
+                    p.c = pk(t.z, t.z);
+                    p.w = pk(t.w, t.w);
+                    s_pk[i] = p;
+                }
             }
             if (tid == 0) {
                 ctl.sector_status = h->status;
@@ -180,28 +230,70 @@ k_sweep_queue(QueueArgs a) {
                 }
             }
             uint32_t i = 0;
+            if constexpr (kF64) {
 #pragma unroll 2
-            for (; i < n_fast; i++) {
-                const float4 t = s_steps[i];
-                const int32_t o = s_offs[i].x;
-                double4 dt;
-                if (kF64) dt = s_dtab[i];
+                for (; i < n_fast; i++) {
+                    const float4 t = s_steps[i];
+                    const int32_t o = s_offs[i].x;
+                    const double4 dt = s_dtab[i];
 #pragma unroll
-                for (int py = 0; py < kPy; py++) {
-                    const float *pf = ep[py] + o;
-                    const float *pb = ep[py] - o;
+                    for (int py = 0; py < kPy; py++) {
+                        const float *pf = ep[py] + o;
+                        const float *pb = ep[py] - o;
 #pragma unroll
-                    for (int px = 0; px < kPx; px++) {
-                        const float hf = __ldg(pf + kTileX * px), hb = __ldg(pb + kTileX * px);
-                        if constexpr (kF64) {
+                        for (int px = 0; px < kPx; px++) {
+                            const float hf = __ldg(pf + kTileX * px), hb = __ldg(pb + kTileX * px);
                             step_f64<kPrec, true>(cf[py][px], hf, hp[py][px], t.y, dt, 0);
                             step_f64<kPrec, true>(cb[py][px], hb, hp[py][px], t.y, dt, 0);
-                        } else {
-                            step_f32<kPrec, true>(cf[py][px], hf, hp[py][px], t, 0);
-                            step_f32<kPrec, true>(cb[py][px], hb, hp[py][px], t, 0);
                         }
                     }
                 }
+            } else {
+                // (forward, backward) pairs: e, the table division and the angle
+                // packed; visibility as 1.0/0.0 so the surface add is a packed
+                // fma (s + 1*w and s + 0*w are exact); maxima stay scalar.
+                f32x2 hp2[kPy][kPx], s2[kPy][kPx];
+#pragma unroll
+                for (int py = 0; py < kPy; py++)
+#pragma unroll
+                    for (int px = 0; px < kPx; px++) {
+                        hp2[py][px] = pk((float)hp[py][px], (float)hp[py][px]);
+                        s2[py][px] = pk(0.0f, 0.0f);
+                    }
+#pragma unroll 2
+                for (; i < n_fast; i++) {
+                    const PackedStep t = s_pk[i];
+                    const int32_t o = s_offs[i].x;
+#pragma unroll
+                    for (int py = 0; py < kPy; py++) {
+                        const float *pf = ep[py] + o;
+                        const float *pb = ep[py] - o;
+#pragma unroll
+                        for (int px = 0; px < kPx; px++) {
+                            const f32x2 e2 = sub2(pk(__ldg(pf + kTileX * px), __ldg(pb + kTileX * px)),
+                                                  hp2[py][px]);
+                            f32x2 q2 = mul2(e2, t.y);
+                            const f32x2 r2 = fma2(t.nd, q2, e2);
+                            q2 = fma2(r2, t.y, q2);
+                            float af, ab;
+                            upk(sub2(q2, t.c), af, ab);
+                            auto &F = cf[py][px];
+                            auto &B = cb[py][px];
+                            s2[py][px] = fma2(pk(gt01(af, F.m), gt01(ab, B.m)), t.w, s2[py][px]);
+                            F.m = fmaxf(af, F.m);  // f32::max: NaN yields the other operand
+                            B.m = fmaxf(ab, B.m);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int py = 0; py < kPy; py++)
+#pragma unroll
+                    for (int px = 0; px < kPx; px++) {
+                        float sf_, sb_;
+                        upk(s2[py][px], sf_, sb_);
+                        cf[py][px].s = sf_;
+                        cb[py][px].s = sb_;
+                    }
             }
             for (; i < n; i++) {
                 const float4 t = s_steps[i];
@@ -318,8 +410,8 @@ cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, cudaStream_t s
     if (rows == 0 || a.tvs_width == 0 || a.n_sectors == 0) return cudaSuccess;
     const bool f64 = precision == TVS_PRECISION_FP64;
     if (!f64 && precision != TVS_PRECISION_EXACT32) return cudaErrorInvalidValue;
-    const size_t smem = 32 + (size_t)a.step_cap * (sizeof(float4) + sizeof(int2) +
-                                                    (f64 ? sizeof(double4) : 0));
+    // ctl + {steps, offs} + FP64 double tables or EXACT32 packed tables (32 B each)
+    const size_t smem = 32 + (size_t)a.step_cap * (sizeof(float4) + sizeof(int2) + 32);
     const PovShape sh = queue_shape();
 #define TVS_Q(X, Y)                                                                    \
     if (sh.px == X && sh.py == Y)                                                      \
