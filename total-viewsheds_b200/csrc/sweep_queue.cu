@@ -135,7 +135,7 @@ __device__ __forceinline__ void step_f64(Chain<kPrec> &c, float h, double hp, fl
     c.m = fmax(a, c.m);
 }
 
-template <int kPrec, int kPx, int kPy>
+template <int kPrec, int kPx, int kPy, bool kPacked>
 __global__ void __launch_bounds__(kThreads)
 k_sweep_queue(QueueArgs a) {
     constexpr bool kF64 = kPrec == TVS_PRECISION_FP64;
@@ -230,12 +230,13 @@ k_sweep_queue(QueueArgs a) {
                 }
             }
             uint32_t i = 0;
-            if constexpr (kF64) {
+            if constexpr (kF64 || !kPacked) {
 #pragma unroll 2
                 for (; i < n_fast; i++) {
                     const float4 t = s_steps[i];
                     const int32_t o = s_offs[i].x;
-                    const double4 dt = s_dtab[i];
+                    double4 dt;
+                    if (kF64) dt = s_dtab[i];
 #pragma unroll
                     for (int py = 0; py < kPy; py++) {
                         const float *pf = ep[py] + o;
@@ -243,8 +244,13 @@ k_sweep_queue(QueueArgs a) {
 #pragma unroll
                         for (int px = 0; px < kPx; px++) {
                             const float hf = __ldg(pf + kTileX * px), hb = __ldg(pb + kTileX * px);
-                            step_f64<kPrec, true>(cf[py][px], hf, hp[py][px], t.y, dt, 0);
-                            step_f64<kPrec, true>(cb[py][px], hb, hp[py][px], t.y, dt, 0);
+                            if constexpr (kF64) {
+                                step_f64<kPrec, true>(cf[py][px], hf, hp[py][px], t.y, dt, 0);
+                                step_f64<kPrec, true>(cb[py][px], hb, hp[py][px], t.y, dt, 0);
+                            } else {
+                                step_f32<kPrec, true>(cf[py][px], hf, hp[py][px], t, 0);
+                                step_f32<kPrec, true>(cb[py][px], hb, hp[py][px], t, 0);
+                            }
                         }
                     }
                 }
@@ -366,9 +372,18 @@ PovShape queue_shape() {
     return v;
 }
 
-template <int kPrec, int kPx, int kPy>
+// Packed f32x2 fast loop (1) or scalar (0): TVS_SWEEP_PACKED overrides the default.
+bool queue_packed() {
+    static bool v = [] {
+        const char *e = getenv("TVS_SWEEP_PACKED");
+        return e ? atoi(e) != 0 : false;
+    }();
+    return v;
+}
+
+template <int kPrec, int kPx, int kPy, bool kPacked>
 cudaError_t launch_queue_t(const QueueArgs &a0, size_t smem, cudaStream_t s) {
-    auto fn = k_sweep_queue<kPrec, kPx, kPy>;
+    auto fn = k_sweep_queue<kPrec, kPx, kPy, kPacked>;
     static int blocks_per_sm = -1;
     static size_t configured_smem = 0;
     int dev = 0, sms = 0;
@@ -413,14 +428,17 @@ cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, cudaStream_t s
     // ctl + {steps, offs} + FP64 double tables or EXACT32 packed tables (32 B each)
     const size_t smem = 32 + (size_t)a.step_cap * (sizeof(float4) + sizeof(int2) + 32);
     const PovShape sh = queue_shape();
+    const bool packed = queue_packed();
 #define TVS_Q(X, Y)                                                                    \
     if (sh.px == X && sh.py == Y)                                                      \
-        return f64 ? launch_queue_t<TVS_PRECISION_FP64, X, Y>(a, smem, s)              \
-                   : launch_queue_t<TVS_PRECISION_EXACT32, X, Y>(a, smem, s);
+        return f64 ? launch_queue_t<TVS_PRECISION_FP64, X, Y, false>(a, smem, s)       \
+               : packed ? launch_queue_t<TVS_PRECISION_EXACT32, X, Y, true>(a, smem, s) \
+                        : launch_queue_t<TVS_PRECISION_EXACT32, X, Y, false>(a, smem, s);
     TVS_Q(1, 1) TVS_Q(2, 1) TVS_Q(2, 2) TVS_Q(8, 1)
 #undef TVS_Q
-    return f64 ? launch_queue_t<TVS_PRECISION_FP64, 4, 1>(a, smem, s)
-               : launch_queue_t<TVS_PRECISION_EXACT32, 4, 1>(a, smem, s);
+    return f64 ? launch_queue_t<TVS_PRECISION_FP64, 4, 1, false>(a, smem, s)
+           : packed ? launch_queue_t<TVS_PRECISION_EXACT32, 4, 1, true>(a, smem, s)
+                    : launch_queue_t<TVS_PRECISION_EXACT32, 4, 1, false>(a, smem, s);
 }
 
 }  // namespace tvs
