@@ -38,6 +38,7 @@ WORKLOADS = {
     "plain_gpu": "plain FP32 GPU form (fBm Hurst 0.75, 15% flat 0 m)",
     "plain_cpu": "plain CPU-runnable form (fBm Hurst 0.8)",
     "large": "large single region (2x2 stitched fBm)",
+    "medium": "profiling stand-in (ridged multifractal, 10% flat 0 m)",
 }
 
 

@@ -164,6 +164,10 @@ CONFIGS = {
                       observer_height=1.65, rings_per_km=5.0),
     "large": dict(index=4, width=7201, scale=30.0, max_line_of_sight=72000,
                   observer_height=1.65, rings_per_km=5.0),
+    # not a benchmark configuration: a 2401^2 stand-in with the precision
+    # form's terrain, sized for multi-pass profiler captures
+    "medium": dict(index=5, width=2401, scale=30.0, max_line_of_sight=24000,
+                   observer_height=1.65, rings_per_km=5.0),
 }
 
 
@@ -180,6 +184,8 @@ def config_dem(name):
         return flatten(ridged_multifractal(w, w, 10, seed, 0.0, 4500.0), 0.10, seed + 100)
     if name == "large":
         return stitched_fbm(w, w, 0.8, seed, 0.0, 6000.0)
+    if name == "medium":
+        return flatten(ridged_multifractal(w, w, 10, seed, 0.0, 4500.0), 0.10, seed + 100)
     raise KeyError(name)
 
 
