@@ -142,9 +142,10 @@ k_sweep_queue(QueueArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     QueueCtl &ctl = *reinterpret_cast<QueueCtl *>(smem);
     float4 *s_steps = reinterpret_cast<float4 *>(smem + sizeof(QueueCtl));
-    int2 *s_offs = reinterpret_cast<int2 *>(s_steps + a.step_cap);
-    double4 *s_dtab = reinterpret_cast<double4 *>(s_offs + a.step_cap);  // FP64 only
-    PackedStep *s_pk = reinterpret_cast<PackedStep *>(s_offs + a.step_cap);  // EXACT32 only
+    // forward DEM-id offset of each step, in bytes (a 64-bit add per base address)
+    long long *s_boff = reinterpret_cast<long long *>(s_steps + a.step_cap);
+    double4 *s_dtab = reinterpret_cast<double4 *>(s_boff + a.step_cap);  // FP64 only
+    PackedStep *s_pk = reinterpret_cast<PackedStep *>(s_boff + a.step_cap);  // EXACT32 only
     const uint32_t tid = threadIdx.y * kTileX + threadIdx.x;
     const uint32_t n_tiles = a.tiles_x * a.tiles_y;
     const uint32_t n_items = n_tiles * a.n_sectors;
@@ -165,7 +166,7 @@ k_sweep_queue(QueueArgs a) {
             for (uint32_t i = tid; i < n; i += kThreads) {
                 const float4 t = gs[i];
                 s_steps[i] = t;
-                s_offs[i] = go[i];
+                s_boff[i] = (long long)go[i].x * (long long)sizeof(float);
                 if (kF64) {
                     s_dtab[i] = a.dtab[(uint64_t)slot * a.step_cap + i];
                 } else {
@@ -234,13 +235,13 @@ k_sweep_queue(QueueArgs a) {
 #pragma unroll 2
                 for (; i < n_fast; i++) {
                     const float4 t = s_steps[i];
-                    const int32_t o = s_offs[i].x;
+                    const long long bo = s_boff[i];
                     double4 dt;
                     if (kF64) dt = s_dtab[i];
 #pragma unroll
                     for (int py = 0; py < kPy; py++) {
-                        const float *pf = ep[py] + o;
-                        const float *pb = ep[py] - o;
+                        const float *pf = (const float *)((const char *)ep[py] + bo);
+                        const float *pb = (const float *)((const char *)ep[py] - bo);
 #pragma unroll
                         for (int px = 0; px < kPx; px++) {
                             const float hf = __ldg(pf + kTileX * px), hb = __ldg(pb + kTileX * px);
@@ -269,11 +270,11 @@ k_sweep_queue(QueueArgs a) {
 #pragma unroll 2
                 for (; i < n_fast; i++) {
                     const PackedStep t = s_pk[i];
-                    const int32_t o = s_offs[i].x;
+                    const long long bo = s_boff[i];
 #pragma unroll
                     for (int py = 0; py < kPy; py++) {
-                        const float *pf = ep[py] + o;
-                        const float *pb = ep[py] - o;
+                        const float *pf = (const float *)((const char *)ep[py] + bo);
+                        const float *pb = (const float *)((const char *)ep[py] - bo);
 #pragma unroll
                         for (int px = 0; px < kPx; px++) {
                             const f32x2 e2 = sub2(pk(__ldg(pf + kTileX * px), __ldg(pb + kTileX * px)),
@@ -303,21 +304,25 @@ k_sweep_queue(QueueArgs a) {
             }
             for (; i < n; i++) {
                 const float4 t = s_steps[i];
-                const int2 o = s_offs[i];
+                const long long bo = s_boff[i];
+                // outside the table-division domain (the zero distances)
+                const int slow = !(t.y >= 0x1p-20f && t.y <= 0x1p20f);
                 double4 dt;
                 if (kF64) dt = s_dtab[i];
 #pragma unroll
                 for (int py = 0; py < kPy; py++) {
+                    const float *pf = (const float *)((const char *)ep[py] + bo);
+                    const float *pb = (const float *)((const char *)ep[py] - bo);
 #pragma unroll
                     for (int px = 0; px < kPx; px++) {
-                        const float hf = __ldg(ep[py] + o.x + kTileX * px);
-                        const float hb = __ldg(ep[py] - o.x + kTileX * px);
+                        const float hf = __ldg(pf + kTileX * px);
+                        const float hb = __ldg(pb + kTileX * px);
                         if constexpr (kF64) {
-                            step_f64<kPrec, false>(cf[py][px], hf, hp[py][px], t.y, dt, o.y);
-                            step_f64<kPrec, false>(cb[py][px], hb, hp[py][px], t.y, dt, o.y);
+                            step_f64<kPrec, false>(cf[py][px], hf, hp[py][px], t.y, dt, slow);
+                            step_f64<kPrec, false>(cb[py][px], hb, hp[py][px], t.y, dt, slow);
                         } else {
-                            step_f32<kPrec, false>(cf[py][px], hf, hp[py][px], t, o.y);
-                            step_f32<kPrec, false>(cb[py][px], hb, hp[py][px], t, o.y);
+                            step_f32<kPrec, false>(cf[py][px], hf, hp[py][px], t, slow);
+                            step_f32<kPrec, false>(cb[py][px], hb, hp[py][px], t, slow);
                         }
                     }
                 }
@@ -425,8 +430,8 @@ cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, cudaStream_t s
     if (rows == 0 || a.tvs_width == 0 || a.n_sectors == 0) return cudaSuccess;
     const bool f64 = precision == TVS_PRECISION_FP64;
     if (!f64 && precision != TVS_PRECISION_EXACT32) return cudaErrorInvalidValue;
-    // ctl + {steps, offs} + FP64 double tables or EXACT32 packed tables (32 B each)
-    const size_t smem = 32 + (size_t)a.step_cap * (sizeof(float4) + sizeof(int2) + 32);
+    // ctl + {steps, byte offsets} + FP64 double tables or EXACT32 packed tables (32 B each)
+    const size_t smem = 32 + (size_t)a.step_cap * (sizeof(float4) + sizeof(long long) + 32);
     const PovShape sh = queue_shape();
     const bool packed = queue_packed();
 #define TVS_Q(X, Y)                                                                    \
