@@ -365,7 +365,7 @@ struct PovShape { int px, py; };
 PovShape queue_shape() {
     static PovShape v = [] {
         const char *e = getenv("TVS_SWEEP_SHAPE");
-        PovShape d{4, 1};
+        PovShape d{2, 1};
         if (!e) return d;
         int x = 0, y = 0;
         if (sscanf(e, "%dx%d", &x, &y) != 2) return d;
@@ -439,11 +439,11 @@ cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, cudaStream_t s
         return f64 ? launch_queue_t<TVS_PRECISION_FP64, X, Y, false>(a, smem, s)       \
                : packed ? launch_queue_t<TVS_PRECISION_EXACT32, X, Y, true>(a, smem, s) \
                         : launch_queue_t<TVS_PRECISION_EXACT32, X, Y, false>(a, smem, s);
-    TVS_Q(1, 1) TVS_Q(2, 1) TVS_Q(2, 2) TVS_Q(8, 1)
+    TVS_Q(1, 1) TVS_Q(4, 1) TVS_Q(2, 2) TVS_Q(8, 1)
 #undef TVS_Q
-    return f64 ? launch_queue_t<TVS_PRECISION_FP64, 4, 1, false>(a, smem, s)
-           : packed ? launch_queue_t<TVS_PRECISION_EXACT32, 4, 1, true>(a, smem, s)
-                    : launch_queue_t<TVS_PRECISION_EXACT32, 4, 1, false>(a, smem, s);
+    return f64 ? launch_queue_t<TVS_PRECISION_FP64, 2, 1, false>(a, smem, s)
+           : packed ? launch_queue_t<TVS_PRECISION_EXACT32, 2, 1, true>(a, smem, s)
+                    : launch_queue_t<TVS_PRECISION_EXACT32, 2, 1, false>(a, smem, s);
 }
 
 }  // namespace tvs
