@@ -190,6 +190,26 @@ void *tvs_stream(const tvs_context *ctx);
 /* Number of kernels the last tvs_device_run_sectors call enqueued. */
 uint64_t tvs_last_launch_count(const tvs_context *ctx);
 
+/* ---- allocation-free form -------------------------------------------- */
+
+/* No counterpart in the reference.  One sector for callers that cannot
+ * allocate device memory when they call: hosts whose device memory belongs to
+ * another allocator (a framework's caching allocator or a fixed pool that must
+ * account for every byte), and real-time callers that forbid allocation after
+ * start-up because an allocation can block or fail at any moment.  Inputs and outputs are the caller's device pointers: d_elevations
+ * (width*height f32), d_cumulative (in/out) and d_total (in/out, nullable),
+ * computable_points_count f32 each.  The sector's intermediate tables live in
+ * a 64 KiB static device array inside the library (held by every GPU that
+ * loads it, until exit); lines of sight longer than ~1590 cells do not fit and
+ * return TVS_ERR_CAPACITY.  Exact f32 only.  The call is synchronous on
+ * `stream` (a cudaStream_t, NULL for the legacy stream).  All calls share the
+ * array and overlapping calls would race: the library serialises its own
+ * calls.  The first call on a device looks up the array's device address:
+ * make it before any stream capture.  Error text: tvs_last_error(NULL). */
+int tvs_compute_sector_noalloc(const tvs_params *params, const float *d_elevations,
+                               uint32_t angle, float *d_cumulative, float *d_total,
+                               void *stream);
+
 /* ---- self-checks ------------------------------------------------------ */
 
 /* Compare the sweep's table-driven division with CUDA's IEEE division

@@ -119,6 +119,7 @@ SIGNATURES = {
     "tvs_last_launch_count": (_U64, [_VP]),
     "tvs_selftest_division": (_INT, [_I32, _U64, _U64, _P(_U64)]),
     "tvs_measure_fp32_issue": (_INT, [_I32, _P(ctypes.c_double)]),
+    "tvs_compute_sector_noalloc": (_INT, [_P(Params), _VP, _U32, _VP, _VP, _VP]),
 }
 
 _lib = None

@@ -454,6 +454,10 @@ int collect_rings(tvs_context *c, uint32_t *rings, uint64_t rings_len, tvs_secto
 
 }  // namespace
 
+// Sets the text tvs_last_error(NULL) returns (used by entry points that have
+// no context).
+void tvs_set_create_error(const std::string &msg) { g_create_error = msg; }
+
 extern "C" {
 
 int tvs_abi_version(void) { return TVS_ABI_VERSION; }
