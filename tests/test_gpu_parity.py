@@ -215,3 +215,32 @@ def test_set_elevations_and_device_path(tvs, oracle, synth):
         eng.device_finish()
         c, t = eng.read_surfaces()
     assert np.array_equal(bits(c), bits(c2)) and np.array_equal(bits(t), bits(t2))
+
+
+def test_mixed64_matches_fp64_oracle(tvs, oracle, dem301):
+    """MIXED64 decides every comparison as the all-FP64 sweep does and sums the
+    surfaces in FP64 in step order, so it equals the FP64 oracle bit for bit."""
+    w, s, los = PLAIN_CPU
+    rpk = 20.0
+    g = oracle.geometry(w, s, los, rpk)
+    c0, r0 = oracle.run_f64(g, dem301, 1.65, rings=True)
+    with tvs.Engine(dem301, w, s, los, rings_per_km=rpk, observer_height=1.65,
+                    precision="mixed64") as eng:
+        c1, _, _ = eng.run()
+        c2, _, r2 = eng.run(rings=True)
+    assert np.array_equal(bits(c0.astype(np.float32)), bits(c1))
+    assert np.array_equal(bits(c1), bits(c2))
+    for a in range(180):
+        assert np.array_equal(r0[a], r2[a]), a
+
+
+@pytest.mark.parametrize("cfg,name", [(PLAIN_GPU, "plain_gpu"), ((2401, 30.0, 24000), "medium")])
+def test_mixed64_equals_fp64_sweep(tvs, synth, cfg, name):
+    """Flat 0 m sea and ridges at 1201^2 and 2401^2: MIXED64 == FP64, all sectors."""
+    w, s, los = cfg
+    z = synth.config_dem(name)
+    with tvs.Engine(z, w, s, los, observer_height=1.65, precision="fp64") as eng:
+        c64, t64, _ = eng.run()
+    with tvs.Engine(z, w, s, los, observer_height=1.65, precision="mixed64") as eng:
+        cm, tm, _ = eng.run()
+    assert np.array_equal(bits(c64), bits(cm)) and np.array_equal(bits(t64), bits(tm))

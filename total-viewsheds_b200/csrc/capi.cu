@@ -36,6 +36,7 @@ struct tvs_context {
     uint32_t *d_done = nullptr;
     uint32_t done_cap = 0;
     int32_t *d_error = nullptr;
+    float *d_hmax = nullptr;  // max |elevation| + |observer height| (MIXED64 window)
     int32_t *d_deltas = nullptr;
     float *d_dists = nullptr;
     // ring output (allocated on first use)
@@ -166,7 +167,7 @@ int derive_geometry(const tvs_params *p, tvs_geometry *g, std::string *msg) {
 
 void free_all(tvs_context *c) {
     void *ptrs[] = {c->d_elev, c->d_cum, c->d_total, c->d_cum64, c->d_trig, c->d_hdr,
-                    c->d_steps, c->d_offs, c->d_dtab, c->d_queue, c->d_done, c->d_error,
+                    c->d_steps, c->d_offs, c->d_dtab, c->d_queue, c->d_done, c->d_error, c->d_hmax,
                     c->d_deltas, c->d_dists, c->d_rings, c->d_spill, c->d_counters, c->d_sf,
                     c->d_sb};
     for (void *p : ptrs)
@@ -357,6 +358,7 @@ int enqueue_sweep(tvs_context *c, uint32_t first, uint32_t count, bool rings) {
         q.done = c->d_done;
         q.done_cap = c->done_cap;
         q.error = c->d_error;
+        q.hmax = c->d_hmax;
         q.spin_limit = 1u << 23;  // ~2-4 s of 256 ns sleeps; a real wait is one item (~1 ms)
         TVS_CUDA(c, tvs::launch_sweep_queue(q, (int)c->p.precision, c->stream));
         c->launches++;
@@ -487,8 +489,6 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
     if (params->precision > TVS_PRECISION_FP64 || params->sweep_kernel > TVS_SWEEP_PLAIN ||
         (params->sweep_kernel == TVS_SWEEP_PLAIN && params->precision != TVS_PRECISION_EXACT32))
         return fail(nullptr, TVS_ERR_INVALID_ARGUMENT, "unsupported precision/sweep-kernel pair");
-    if (params->precision == TVS_PRECISION_MIXED64)
-        return fail(nullptr, TVS_ERR_INVALID_ARGUMENT, "MIXED64 precision is not available yet");
     uint32_t rb = params->tvs_row_begin, re = params->tvs_row_end;
     if (rb == 0 && re == 0) re = g.tvs_height;
     if (rb > re || re > g.tvs_height)
@@ -540,12 +540,13 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
         {(void **)&c->d_queue, sizeof(uint32_t)},
         {(void **)&c->d_done, (size_t)std::max<uint32_t>(c->done_cap, 1) * sizeof(uint32_t)},
         {(void **)&c->d_error, sizeof(int32_t)},
+        {(void **)&c->d_hmax, sizeof(float)},
         {(void **)&c->d_deltas, (size_t)slots * bds * sizeof(int32_t)},
         {(void **)&c->d_dists, (size_t)slots * bds * sizeof(float)},
     };
     for (auto &a : allocs)
         if ((e = cudaMalloc(a.p, a.bytes)) != cudaSuccess) return bail(e, "cudaMalloc");
-    if (params->precision == TVS_PRECISION_FP64 &&
+    if (params->precision != TVS_PRECISION_EXACT32 &&
         (e = cudaMalloc(&c->d_cum64, count * sizeof(double))) != cudaSuccess)
         return bail(e, "cudaMalloc");
     // Per-sector trigonometry on the host (glibc, as Rust std on linux-gnu):
@@ -568,6 +569,10 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
         return bail(e, "cudaMemcpy elevations");
     if ((e = cudaMemset(c->d_elev + g.size, 0, tvs::kElevationPad * sizeof(float))) != cudaSuccess)
         return bail(e, "cudaMemset elevation padding");
+    if ((e = tvs::launch_max_abs(c->d_elev, g.size, params->observer_height, c->d_hmax, 0)) !=
+            cudaSuccess ||
+        (e = cudaDeviceSynchronize()) != cudaSuccess)
+        return bail(e, "elevation range");
     if ((e = cudaMemset(c->d_hdr, 0, slots * sizeof(tvs::ShapeHeader))) != cudaSuccess ||
         (e = cudaMemset(c->d_error, 0, sizeof(int32_t))) != cudaSuccess ||
         (e = cudaMemset(c->d_cum, 0, count * sizeof(float))) != cudaSuccess ||
@@ -600,6 +605,9 @@ int tvs_set_elevations(tvs_context *ctx, const float *elevations, uint64_t n) {
     TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
     TVS_CUDA(ctx, cudaMemcpyAsync(ctx->d_elev, elevations, n * sizeof(float),
                                   cudaMemcpyHostToDevice, ctx->stream));
+    if (ctx->p.precision == TVS_PRECISION_MIXED64)
+        TVS_CUDA(ctx, tvs::launch_max_abs(ctx->d_elev, n, ctx->p.observer_height, ctx->d_hmax,
+                                          ctx->stream));
     return TVS_OK;
 }
 
@@ -684,9 +692,9 @@ int tvs_compute_sector(tvs_context *ctx, uint32_t angle, float *cumulative_surfa
         return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "rings_len is smaller than one sector's slots");
     TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
     const uint64_t count = ctx->g.computable_points_count;
-    if (ctx->p.precision == TVS_PRECISION_FP64)
+    if (ctx->p.precision != TVS_PRECISION_EXACT32)
         return fail(ctx, TVS_ERR_INVALID_ARGUMENT,
-                    "tvs_compute_sector keeps f32 cumulative surfaces; use tvs_run for FP64");
+                    "tvs_compute_sector keeps f32 cumulative surfaces; use tvs_run for FP64/MIXED64");
     if (count)
         TVS_CUDA(ctx, cudaMemcpyAsync(ctx->d_cum, cumulative_surfaces, count * sizeof(float),
                                       cudaMemcpyHostToDevice, ctx->stream));
@@ -823,7 +831,7 @@ int tvs_run(tvs_context *ctx, float *cumulative_out, float *total_out, int want_
             }
         return tvs_read_surfaces(ctx, cumulative_out, total_out);
     }
-    if (ctx->p.precision == TVS_PRECISION_FP64 && !ctx->d_cum64)
+    if (ctx->p.precision != TVS_PRECISION_EXACT32 && !ctx->d_cum64)
         return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "FP64 context without FP64 accumulator");
     rc = ensure_rings(ctx);
     if (rc) return rc;

@@ -461,7 +461,24 @@ __global__ void __launch_bounds__(256) k_ffma_issue(float *out, int iters, float
     if (s == 1234.5f) out[0] = s;  // keeps the chains live
 }
 
+// out[0] = max |x| + |add| (non-negative floats order as their bit patterns).
+__global__ void k_max_abs(const float *x, uint64_t n, float add, unsigned int *out) {
+    float m = 0.0f;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        m = fmaxf(m, fabsf(x[i]));
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(__fadd_ru(m, fabsf(add))));
+}
+
 }  // namespace
+
+cudaError_t launch_max_abs(const float *x, uint64_t n, float add, float *out, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(float), s);
+    if (e != cudaSuccess) return e;
+    k_max_abs<<<148 * 4, 256, 0, s>>>(x, n, add, reinterpret_cast<unsigned int *>(out));
+    return cudaGetLastError();
+}
 
 cudaError_t measure_fp32_issue(double *instructions_per_second) {
     int dev = 0, sms = 0;
@@ -500,7 +517,9 @@ cudaError_t launch_sweep_engine(const SweepArgs &a, int precision, cudaStream_t 
     const size_t smem = (size_t)a.step_cap * (sizeof(float4) + sizeof(int2));
     const bool rings = a.rings != nullptr;
     void (*fn)(SweepArgs);
-    if (precision == TVS_PRECISION_FP64)
+    // MIXED64 decides every comparison as the FP64 sweep does, so the FP64
+    // kernel produces its ring records and surfaces
+    if (precision == TVS_PRECISION_FP64 || precision == TVS_PRECISION_MIXED64)
         fn = rings ? k_sweep_fp64<true> : k_sweep_fp64<false>;
     else if (precision == TVS_PRECISION_EXACT32)
         fn = rings ? k_sweep_exact32<true> : k_sweep_exact32<false>;

@@ -110,6 +110,18 @@ template <> struct Chain<TVS_PRECISION_FP64> {
     double m, s;
     __device__ void init() { m = -2000.0; s = 0.0; }
 };
+// MIXED64: m is the FP64 running maximum (exact when `valid`), s the FP64
+// surface; m32 is the FP32 estimate of the angle at the maximum, gm the part
+// of the decision window that belongs to it, j the step of the maximum.
+template <> struct Chain<TVS_PRECISION_MIXED64> {
+    double m, s;
+    float m32, gm;
+    int32_t j;
+    bool valid;
+    __device__ void init() {
+        m = -2000.0; s = 0.0; m32 = -2000.0f; gm = 0.0f; j = -1; valid = true;
+    }
+};
 
 template <int kPrec, bool kFast>
 __device__ __forceinline__ void step_f32(Chain<kPrec> &c, float h, float hp, const float4 &t,
@@ -138,7 +150,8 @@ __device__ __forceinline__ void step_f64(Chain<kPrec> &c, float h, double hp, fl
 template <int kPrec, int kPx, int kPy, bool kPacked>
 __global__ void __launch_bounds__(kThreads)
 k_sweep_queue(QueueArgs a) {
-    constexpr bool kF64 = kPrec == TVS_PRECISION_FP64;
+    constexpr bool kMix = kPrec == TVS_PRECISION_MIXED64;
+    constexpr bool kF64 = kPrec == TVS_PRECISION_FP64 || kMix;  // FP64 tables and surfaces
     extern __shared__ __align__(16) unsigned char smem[];
     QueueCtl &ctl = *reinterpret_cast<QueueCtl *>(smem);
     float4 *s_steps = reinterpret_cast<float4 *>(smem + sizeof(QueueCtl));
@@ -163,9 +176,18 @@ k_sweep_queue(QueueArgs a) {
             const uint32_t n = h->n_steps;
             const float4 *gs = a.steps + (uint64_t)slot * a.step_cap;
             const int2 *go = a.offs + (uint64_t)slot * a.step_cap;
+            const float hmax = kMix ? *a.hmax : 0.0f;
             for (uint32_t i = tid; i < n; i += kThreads) {
                 const float4 t = gs[i];
                 s_steps[i] = t;
+                if (kMix) {
+                    // decision window of the FP32 estimate at this step: at least 4x
+                    // the bound 2^-22 (|a| + d/R + hmax/d) on |estimate - FP64 angle|
+                    // (the |a| part is carried with the running maximum)
+                    const float g = __fadd_rn(__fmul_rn(0x1p-20f, __fadd_rn(t.z, __fmul_rn(hmax, t.x))),
+                                              0x1p-90f);
+                    s_steps[i] = make_float4(t.x, t.y, -t.z, g);
+                }
                 s_boff[i] = (long long)go[i].x * (long long)sizeof(float);
                 if (kF64) {
                     s_dtab[i] = a.dtab[(uint64_t)slot * a.step_cap + i];
@@ -214,6 +236,7 @@ k_sweep_queue(QueueArgs a) {
             const float *ep[kPy];
             using HP = typename std::conditional<kF64, double, float>::type;
             HP hp[kPy][kPx];
+            float hp32[kPy][kPx];
             Chain<kPrec> cf[kPy][kPx], cb[kPy][kPx];
 #pragma unroll
             for (int py = 0; py < kPy; py++) {
@@ -226,12 +249,102 @@ k_sweep_queue(QueueArgs a) {
                     const float h0 = __ldg(ep[py] + kTileX * px);
                     if (kF64) hp[py][px] = (HP)__dadd_rn((double)h0, (double)a.observer_height);
                     else hp[py][px] = (HP)__fadd_rn(h0, a.observer_height);  // kernel.rs:134
+                    hp32[py][px] = __fadd_rn(h0, a.observer_height);
                     cf[py][px].init();
                     cb[py][px].init();
                 }
             }
             uint32_t i = 0;
-            if constexpr (kF64 || !kPacked) {
+            if constexpr (kMix) {
+                // FP32 estimate per sample; FP64 only for comparisons inside the
+                // window, and for the exact maximum they need (recomputed from
+                // the step of the maximum).
+                for (; i < n_fast; i++) {
+                    const float4 t = s_steps[i];
+                    const long long bo = s_boff[i];
+                    const double4 dt = s_dtab[i];
+                    bool any_amb = false;
+                    float hv[kPy][kPx][2], av[kPy][kPx][2];
+                    bool amb[kPy][kPx][2];
+#pragma unroll
+                    for (int py = 0; py < kPy; py++) {
+                        const float *pf = (const float *)((const char *)ep[py] + bo);
+                        const float *pb = (const float *)((const char *)ep[py] - bo);
+#pragma unroll
+                        for (int px = 0; px < kPx; px++) {
+#pragma unroll
+                            for (int dir = 0; dir < 2; dir++) {
+                                auto &c = dir ? cb[py][px] : cf[py][px];
+                                const float h = __ldg((dir ? pb : pf) + kTileX * px);
+                                const float e = __fsub_rn(h, hp32[py][px]);
+                                const float ah = __fmaf_rn(e, t.x, t.z);
+                                const float dd = __fsub_rn(ah, c.m32);
+                                const bool am = fabsf(dd) <= __fadd_rn(t.w, c.gm);
+                                if (!am && dd > 0.0f) {  // surely visible
+                                    c.m32 = ah;
+                                    c.gm = __fmaf_rn(fabsf(ah), 0x1p-19f, t.w);
+                                    c.j = (int32_t)i;
+                                    c.valid = false;
+                                    c.s = __dadd_rn(c.s, dt.z);
+                                }
+                                hv[py][px][dir] = h;
+                                av[py][px][dir] = ah;
+                                amb[py][px][dir] = am;
+                                any_amb |= am;
+                            }
+                        }
+                    }
+                    if (__any_sync(0xffffffffu, any_amb)) {
+#pragma unroll
+                        for (int py = 0; py < kPy; py++)
+#pragma unroll
+                            for (int px = 0; px < kPx; px++)
+#pragma unroll
+                                for (int dir = 0; dir < 2; dir++) {
+                                    if (!amb[py][px][dir]) continue;
+                                    auto &c = dir ? cb[py][px] : cf[py][px];
+                                    if (!c.valid) {  // the exact FP64 angle at the maximum
+                                        const uint32_t j = (uint32_t)c.j;
+                                        const long long bj = s_boff[j];
+                                        const float *pj = (const float *)((const char *)ep[py] +
+                                                                          (dir ? -bj : bj));
+                                        const double ej =
+                                            __dsub_rn((double)__ldg(pj + kTileX * px), hp[py][px]);
+                                        const double4 dj = s_dtab[j];
+                                        c.m = __dsub_rn(div_table64(ej, dj.x, (double)s_steps[j].y), dj.y);
+                                        c.valid = true;
+                                    }
+                                    const double e64 = __dsub_rn((double)hv[py][px][dir], hp[py][px]);
+                                    const double a64 = __dsub_rn(div_table64(e64, dt.x, (double)t.y), dt.y);
+                                    if (a64 > c.m) {
+                                        c.m = a64;
+                                        c.valid = true;
+                                        c.m32 = av[py][px][dir];
+                                        c.gm = __fmaf_rn(fabsf(c.m32), 0x1p-19f, t.w);
+                                        c.j = (int32_t)i;
+                                        c.s = __dadd_rn(c.s, dt.z);
+                                    }
+                                }
+                    }
+                }
+                // the exact maximum before the IEEE-division tail
+#pragma unroll
+                for (int py = 0; py < kPy; py++)
+#pragma unroll
+                    for (int px = 0; px < kPx; px++)
+#pragma unroll
+                        for (int dir = 0; dir < 2; dir++) {
+                            auto &c = dir ? cb[py][px] : cf[py][px];
+                            if (c.valid) continue;
+                            const uint32_t j = (uint32_t)c.j;
+                            const long long bj = s_boff[j];
+                            const float *pj = (const float *)((const char *)ep[py] + (dir ? -bj : bj));
+                            const double ej = __dsub_rn((double)__ldg(pj + kTileX * px), hp[py][px]);
+                            const double4 dj = s_dtab[j];
+                            c.m = __dsub_rn(div_table64(ej, dj.x, (double)s_steps[j].y), dj.y);
+                            c.valid = true;
+                        }
+            } else if constexpr (kF64 || !kPacked) {
 #pragma unroll 2
                 for (; i < n_fast; i++) {
                     const float4 t = s_steps[i];
@@ -428,20 +541,24 @@ uint32_t queue_tiles_bound(uint32_t tvs_width, uint32_t rows) {
 cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, cudaStream_t s) {
     const uint32_t rows = a.row_end - a.row_begin;
     if (rows == 0 || a.tvs_width == 0 || a.n_sectors == 0) return cudaSuccess;
+    const bool mix = precision == TVS_PRECISION_MIXED64;
     const bool f64 = precision == TVS_PRECISION_FP64;
-    if (!f64 && precision != TVS_PRECISION_EXACT32) return cudaErrorInvalidValue;
+    if (!f64 && !mix && precision != TVS_PRECISION_EXACT32) return cudaErrorInvalidValue;
+    if (mix && !a.hmax) return cudaErrorInvalidValue;
     // ctl + {steps, byte offsets} + FP64 double tables or EXACT32 packed tables (32 B each)
     const size_t smem = 32 + (size_t)a.step_cap * (sizeof(float4) + sizeof(long long) + 32);
     const PovShape sh = queue_shape();
     const bool packed = queue_packed();
 #define TVS_Q(X, Y)                                                                    \
     if (sh.px == X && sh.py == Y)                                                      \
-        return f64 ? launch_queue_t<TVS_PRECISION_FP64, X, Y, false>(a, smem, s)       \
+        return mix ? launch_queue_t<TVS_PRECISION_MIXED64, X, Y, false>(a, smem, s)    \
+               : f64 ? launch_queue_t<TVS_PRECISION_FP64, X, Y, false>(a, smem, s)     \
                : packed ? launch_queue_t<TVS_PRECISION_EXACT32, X, Y, true>(a, smem, s) \
                         : launch_queue_t<TVS_PRECISION_EXACT32, X, Y, false>(a, smem, s);
     TVS_Q(1, 1) TVS_Q(4, 1) TVS_Q(2, 2) TVS_Q(8, 1)
 #undef TVS_Q
-    return f64 ? launch_queue_t<TVS_PRECISION_FP64, 2, 1, false>(a, smem, s)
+    return mix ? launch_queue_t<TVS_PRECISION_MIXED64, 2, 1, false>(a, smem, s)
+           : f64 ? launch_queue_t<TVS_PRECISION_FP64, 2, 1, false>(a, smem, s)
            : packed ? launch_queue_t<TVS_PRECISION_EXACT32, 2, 1, true>(a, smem, s)
                     : launch_queue_t<TVS_PRECISION_EXACT32, 2, 1, false>(a, smem, s);
 }

@@ -123,6 +123,7 @@ struct QueueArgs {
     uint32_t done_cap;
     int32_t *error;                    // TVS_ERR_TIMEOUT when a wait gives up
     uint32_t spin_limit;
+    const float *hmax;                 // MIXED64: max |elevation| + |observer height|
 };
 
 struct PlainArgs {
@@ -170,6 +171,8 @@ uint32_t queue_tiles_bound(uint32_t tvs_width, uint32_t rows);
 cudaError_t launch_combine(float *cum, float *total, const float *sf, const float *sb,
                            uint64_t n, cudaStream_t s);
 cudaError_t measure_fp32_issue(double *instructions_per_second);
+// out[0] = max |x[i]| + |add| over n floats (out must hold 1 float).
+cudaError_t launch_max_abs(const float *x, uint64_t n, float add, float *out, cudaStream_t s);
 cudaError_t launch_selftest_division(uint64_t n, uint64_t seed, unsigned long long *mismatches,
                                      cudaStream_t s);
 
