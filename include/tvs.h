@@ -183,6 +183,9 @@ int tvs_device_sweep_sectors(tvs_context *ctx, uint32_t first_angle, uint32_t co
 int tvs_device_finish(tvs_context *ctx);
 /* Copy the device surfaces to the host (either pointer nullable). */
 int tvs_read_surfaces(tvs_context *ctx, float *cumulative_out, float *total_out);
+/* MIXED64: number of sample comparisons re-decided in FP64 since the last
+ * reset (reset != 0 clears the counter after reading). */
+int tvs_read_rechecks(tvs_context *ctx, uint64_t *count, int reset);
 /* Device pointer of the float32 cumulative surfaces, for zero-copy callers. */
 const float *tvs_device_cumulative(const tvs_context *ctx);
 /* The context's CUDA stream (a cudaStream_t), for callers that time on it. */

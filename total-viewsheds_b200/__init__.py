@@ -115,6 +115,7 @@ SIGNATURES = {
     "tvs_device_finish": (_INT, [_VP]),
     "tvs_read_surfaces": (_INT, [_VP, _VP, _VP]),
     "tvs_device_cumulative": (_VP, [_VP]),
+    "tvs_read_rechecks": (_INT, [_VP, _P(_U64), _INT]),
     "tvs_stream": (_VP, [_VP]),
     "tvs_last_launch_count": (_U64, [_VP]),
     "tvs_selftest_division": (_INT, [_I32, _U64, _U64, _P(_U64)]),
@@ -295,6 +296,12 @@ class Engine:
 
     def stream(self):
         return lib().tvs_stream(self.ctx)
+
+    def read_rechecks(self, reset=True):
+        """MIXED64: comparisons re-decided in FP64 since the last reset."""
+        v = ctypes.c_uint64()
+        self._check(lib().tvs_read_rechecks(self.ctx, ctypes.byref(v), 1 if reset else 0))
+        return v.value
 
     def last_launch_count(self):
         return lib().tvs_last_launch_count(self.ctx)

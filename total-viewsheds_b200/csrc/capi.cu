@@ -37,6 +37,7 @@ struct tvs_context {
     uint32_t done_cap = 0;
     int32_t *d_error = nullptr;
     float *d_hmax = nullptr;  // max |elevation| + |observer height| (MIXED64 window)
+    unsigned long long *d_rechecks = nullptr;  // MIXED64 FP64 re-decisions
     int32_t *d_deltas = nullptr;
     float *d_dists = nullptr;
     // ring output (allocated on first use)
@@ -168,6 +169,7 @@ int derive_geometry(const tvs_params *p, tvs_geometry *g, std::string *msg) {
 void free_all(tvs_context *c) {
     void *ptrs[] = {c->d_elev, c->d_cum, c->d_total, c->d_cum64, c->d_trig, c->d_hdr,
                     c->d_steps, c->d_offs, c->d_dtab, c->d_queue, c->d_done, c->d_error, c->d_hmax,
+                    c->d_rechecks,
                     c->d_deltas, c->d_dists, c->d_rings, c->d_spill, c->d_counters, c->d_sf,
                     c->d_sb};
     for (void *p : ptrs)
@@ -359,6 +361,7 @@ int enqueue_sweep(tvs_context *c, uint32_t first, uint32_t count, bool rings) {
         q.done_cap = c->done_cap;
         q.error = c->d_error;
         q.hmax = c->d_hmax;
+        q.rechecks = c->d_rechecks;
         q.spin_limit = 1u << 23;  // ~2-4 s of 256 ns sleeps; a real wait is one item (~1 ms)
         TVS_CUDA(c, tvs::launch_sweep_queue(q, (int)c->p.precision, c->stream));
         c->launches++;
@@ -541,6 +544,7 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
         {(void **)&c->d_done, (size_t)std::max<uint32_t>(c->done_cap, 1) * sizeof(uint32_t)},
         {(void **)&c->d_error, sizeof(int32_t)},
         {(void **)&c->d_hmax, sizeof(float)},
+        {(void **)&c->d_rechecks, sizeof(unsigned long long)},
         {(void **)&c->d_deltas, (size_t)slots * bds * sizeof(int32_t)},
         {(void **)&c->d_dists, (size_t)slots * bds * sizeof(float)},
     };
@@ -575,6 +579,7 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
         return bail(e, "elevation range");
     if ((e = cudaMemset(c->d_hdr, 0, slots * sizeof(tvs::ShapeHeader))) != cudaSuccess ||
         (e = cudaMemset(c->d_error, 0, sizeof(int32_t))) != cudaSuccess ||
+        (e = cudaMemset(c->d_rechecks, 0, sizeof(unsigned long long))) != cudaSuccess ||
         (e = cudaMemset(c->d_cum, 0, count * sizeof(float))) != cudaSuccess ||
         (e = cudaMemset(c->d_total, 0, count * sizeof(float))) != cudaSuccess)
         return bail(e, "cudaMemset");
@@ -807,6 +812,17 @@ int tvs_read_surfaces(tvs_context *ctx, float *cumulative_out, float *total_out)
 }
 
 const float *tvs_device_cumulative(const tvs_context *ctx) { return ctx ? ctx->d_cum : nullptr; }
+
+int tvs_read_rechecks(tvs_context *ctx, uint64_t *count, int reset) {
+    if (!ctx || !count) return TVS_ERR_INVALID_ARGUMENT;
+    TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
+    unsigned long long v = 0;
+    TVS_CUDA(ctx, cudaMemcpyAsync(&v, ctx->d_rechecks, sizeof v, cudaMemcpyDeviceToHost, ctx->stream));
+    TVS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (reset) TVS_CUDA(ctx, cudaMemset(ctx->d_rechecks, 0, sizeof v));
+    *count = v;
+    return TVS_OK;
+}
 
 void *tvs_stream(const tvs_context *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 

@@ -110,17 +110,15 @@ template <> struct Chain<TVS_PRECISION_FP64> {
     double m, s;
     __device__ void init() { m = -2000.0; s = 0.0; }
 };
-// MIXED64: m is the FP64 running maximum (exact when `valid`), s the FP64
-// surface; m32 is the FP32 estimate of the angle at the maximum, gm the part
-// of the decision window that belongs to it, j the step of the maximum.
+// MIXED64: m is the FP64 running maximum, s the FP64 surface; m32 is the FP32
+// estimate of the angle at the maximum and gm the part of the decision window
+// that belongs to it.  j >= 0: m is stale and is recomputed from step j when a
+// comparison needs it; j < 0: m is exact.
 template <> struct Chain<TVS_PRECISION_MIXED64> {
     double m, s;
     float m32, gm;
     int32_t j;
-    bool valid;
-    __device__ void init() {
-        m = -2000.0; s = 0.0; m32 = -2000.0f; gm = 0.0f; j = -1; valid = true;
-    }
+    __device__ void init() { m = -2000.0; s = 0.0; m32 = -2000.0f; gm = 0.0f; j = -1; }
 };
 
 template <int kPrec, bool kFast>
@@ -147,8 +145,15 @@ __device__ __forceinline__ void step_f64(Chain<kPrec> &c, float h, double hp, fl
     c.m = fmax(a, c.m);
 }
 
+// MIXED64 carries 7 registers of state per chain; with one or two points of
+// view per thread it is held to 64 registers (4 CTAs per SM).
+template <int kPrec, int kPx, int kPy>
+constexpr int queue_min_blocks() {
+    return (kPrec == TVS_PRECISION_MIXED64 && kPx * kPy <= 2) ? 4 : 1;
+}
+
 template <int kPrec, int kPx, int kPy, bool kPacked>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, (queue_min_blocks<kPrec, kPx, kPy>()))
 k_sweep_queue(QueueArgs a) {
     constexpr bool kMix = kPrec == TVS_PRECISION_MIXED64;
     constexpr bool kF64 = kPrec == TVS_PRECISION_FP64 || kMix;  // FP64 tables and surfaces
@@ -259,13 +264,18 @@ k_sweep_queue(QueueArgs a) {
                 // FP32 estimate per sample; FP64 only for comparisons inside the
                 // window, and for the exact maximum they need (recomputed from
                 // the step of the maximum).
+                auto exact_angle = [&](int py, int px, int dir, uint32_t k) -> double {
+                    const long long bk = s_boff[k];
+                    const float *pk_ = (const float *)((const char *)ep[py] + (dir ? -bk : bk));
+                    const double ek = __dsub_rn((double)__ldg(pk_ + kTileX * px), hp[py][px]);
+                    const double4 dk = s_dtab[k];
+                    return __dsub_rn(div_table64(ek, dk.x, (double)s_steps[k].y), dk.y);
+                };
                 for (; i < n_fast; i++) {
                     const float4 t = s_steps[i];
                     const long long bo = s_boff[i];
-                    const double4 dt = s_dtab[i];
-                    bool any_amb = false;
-                    float hv[kPy][kPx][2], av[kPy][kPx][2];
-                    bool amb[kPy][kPx][2];
+                    const double w64 = s_dtab[i].z;
+                    uint32_t amb = 0;  // one bit per chain
 #pragma unroll
                     for (int py = 0; py < kPy; py++) {
                         const float *pf = (const float *)((const char *)ep[py] + bo);
@@ -276,53 +286,42 @@ k_sweep_queue(QueueArgs a) {
                             for (int dir = 0; dir < 2; dir++) {
                                 auto &c = dir ? cb[py][px] : cf[py][px];
                                 const float h = __ldg((dir ? pb : pf) + kTileX * px);
-                                const float e = __fsub_rn(h, hp32[py][px]);
-                                const float ah = __fmaf_rn(e, t.x, t.z);
+                                const float ah = __fmaf_rn(__fsub_rn(h, hp32[py][px]), t.x, t.z);
                                 const float dd = __fsub_rn(ah, c.m32);
                                 const bool am = fabsf(dd) <= __fadd_rn(t.w, c.gm);
                                 if (!am && dd > 0.0f) {  // surely visible
                                     c.m32 = ah;
                                     c.gm = __fmaf_rn(fabsf(ah), 0x1p-19f, t.w);
                                     c.j = (int32_t)i;
-                                    c.valid = false;
-                                    c.s = __dadd_rn(c.s, dt.z);
+                                    c.s = __dadd_rn(c.s, w64);
                                 }
-                                hv[py][px][dir] = h;
-                                av[py][px][dir] = ah;
-                                amb[py][px][dir] = am;
-                                any_amb |= am;
+                                amb |= (uint32_t)am << ((py * kPx + px) * 2 + dir);
                             }
                         }
                     }
-                    if (__any_sync(0xffffffffu, any_amb)) {
+                    if (__any_sync(0xffffffffu, amb != 0)) {
+                        if (amb && a.rechecks) atomicAdd(a.rechecks, (unsigned long long)__popc(amb));
 #pragma unroll
                         for (int py = 0; py < kPy; py++)
 #pragma unroll
                             for (int px = 0; px < kPx; px++)
 #pragma unroll
                                 for (int dir = 0; dir < 2; dir++) {
-                                    if (!amb[py][px][dir]) continue;
+                                    if (!((amb >> ((py * kPx + px) * 2 + dir)) & 1u)) continue;
                                     auto &c = dir ? cb[py][px] : cf[py][px];
-                                    if (!c.valid) {  // the exact FP64 angle at the maximum
-                                        const uint32_t j = (uint32_t)c.j;
-                                        const long long bj = s_boff[j];
-                                        const float *pj = (const float *)((const char *)ep[py] +
-                                                                          (dir ? -bj : bj));
-                                        const double ej =
-                                            __dsub_rn((double)__ldg(pj + kTileX * px), hp[py][px]);
-                                        const double4 dj = s_dtab[j];
-                                        c.m = __dsub_rn(div_table64(ej, dj.x, (double)s_steps[j].y), dj.y);
-                                        c.valid = true;
+                                    if (c.j >= 0) {  // the exact FP64 angle at the maximum
+                                        c.m = exact_angle(py, px, dir, (uint32_t)c.j);
+                                        c.j = -1;
                                     }
-                                    const double e64 = __dsub_rn((double)hv[py][px][dir], hp[py][px]);
-                                    const double a64 = __dsub_rn(div_table64(e64, dt.x, (double)t.y), dt.y);
+                                    const double a64 = exact_angle(py, px, dir, i);
                                     if (a64 > c.m) {
                                         c.m = a64;
-                                        c.valid = true;
-                                        c.m32 = av[py][px][dir];
+                                        const long long bi = dir ? -bo : bo;
+                                        const float h = __ldg((const float *)((const char *)ep[py] + bi) +
+                                                              kTileX * px);
+                                        c.m32 = __fmaf_rn(__fsub_rn(h, hp32[py][px]), t.x, t.z);
                                         c.gm = __fmaf_rn(fabsf(c.m32), 0x1p-19f, t.w);
-                                        c.j = (int32_t)i;
-                                        c.s = __dadd_rn(c.s, dt.z);
+                                        c.s = __dadd_rn(c.s, w64);
                                     }
                                 }
                     }
@@ -335,14 +334,9 @@ k_sweep_queue(QueueArgs a) {
 #pragma unroll
                         for (int dir = 0; dir < 2; dir++) {
                             auto &c = dir ? cb[py][px] : cf[py][px];
-                            if (c.valid) continue;
-                            const uint32_t j = (uint32_t)c.j;
-                            const long long bj = s_boff[j];
-                            const float *pj = (const float *)((const char *)ep[py] + (dir ? -bj : bj));
-                            const double ej = __dsub_rn((double)__ldg(pj + kTileX * px), hp[py][px]);
-                            const double4 dj = s_dtab[j];
-                            c.m = __dsub_rn(div_table64(ej, dj.x, (double)s_steps[j].y), dj.y);
-                            c.valid = true;
+                            if (c.j < 0) continue;
+                            c.m = exact_angle(py, px, dir, (uint32_t)c.j);
+                            c.j = -1;
                         }
             } else if constexpr (kF64 || !kPacked) {
 #pragma unroll 2

@@ -124,6 +124,7 @@ struct QueueArgs {
     int32_t *error;                    // TVS_ERR_TIMEOUT when a wait gives up
     uint32_t spin_limit;
     const float *hmax;                 // MIXED64: max |elevation| + |observer height|
+    unsigned long long *rechecks;      // MIXED64: FP64 re-decisions (nullable)
 };
 
 struct PlainArgs {
