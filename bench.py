@@ -258,6 +258,8 @@ def main():
     for _ in range(args.warmup):
         full_tvs()
         eng.device_finish()
+    if args.precision == "mixed64":
+        eng.read_rechecks(reset=True)
 
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
     launches0 = eng.last_launch_count()
@@ -276,6 +278,7 @@ def main():
     eng.device_finish()
     barrier()
     gpu_launches = eng.last_launch_count() - launches0
+    rechecks = eng.read_rechecks(reset=True) if args.precision == "mixed64" else None
     step_ms = [ev[k][0].elapsed_time(ev[k][2]) for k in range(args.steps)]
     shape_ms = [ev[k][0].elapsed_time(ev[k][1]) for k in range(args.steps)]
     sweep_ms = [ev[k][1].elapsed_time(ev[k][2]) for k in range(args.steps)]
@@ -380,6 +383,8 @@ def main():
                 "los_samples_per_tvs": ref_samples,
                 "evaluated_samples_per_tvs": eval_samples,
                 "evaluated_samples_per_s": world * args.steps * eval_samples / (total_ms * 1e-3),
+                "fp64_rechecks_per_evaluated_sample":
+                    None if rechecks is None else rechecks / (args.steps * eval_samples),
                 "note": "delta-table entries the reference leaves at 0 after the first two are "
                         "provably no-ops and are not evaluated; samples counted as the reference "
                         "loop counts them",
