@@ -393,7 +393,8 @@ def main():
                 "bound": "fp32_issue", "achieved": achieved / 1e12,
                 "peak": fp32_peak / 1e12, "unit": "Tinstr/s",
                 "frac": achieved / fp32_peak, "traffic": traffic,
-                "kernel": "k_sweep_exact32 (one launch: 180 sectors)",
+                "kernel": f"k_sweep_queue<{args.precision}> (one persistent launch: 180 sectors)"
+                          if args.kernel == "engine" else "k_sweep_plain (one launch per sector)",
                 "algorithmic_work": "5 FP32 instructions per evaluated sample (sub, fma, "
                                     "setp, max, predicated add)",
                 "peak_source": "measured: FFMA issue microbenchmark on this GPU "
