@@ -383,6 +383,8 @@ def main():
                 "los_samples_per_tvs": ref_samples,
                 "evaluated_samples_per_tvs": eval_samples,
                 "evaluated_samples_per_s": world * args.steps * eval_samples / (total_ms * 1e-3),
+                "hbm_bytes_context": eng.device_bytes(),
+                "ring_buffer_bytes_per_sector": int(g.ring_slots_per_sector * 4),
                 "fp64_rechecks_per_evaluated_sample":
                     None if rechecks is None else rechecks / (args.steps * eval_samples),
                 "note": "delta-table entries the reference leaves at 0 after the first two are "

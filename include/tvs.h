@@ -192,6 +192,9 @@ const float *tvs_device_cumulative(const tvs_context *ctx);
 void *tvs_stream(const tvs_context *ctx);
 /* Number of kernels the last tvs_device_run_sectors call enqueued. */
 uint64_t tvs_last_launch_count(const tvs_context *ctx);
+/* Bytes of device memory the context holds (its peak: buffers are only ever
+ * added, the ring buffers on the first run that asks for ring records). */
+uint64_t tvs_device_bytes(const tvs_context *ctx);
 
 /* ---- allocation-free form -------------------------------------------- */
 

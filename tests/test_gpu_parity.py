@@ -244,3 +244,15 @@ def test_mixed64_equals_fp64_sweep(tvs, synth, cfg, name):
     with tvs.Engine(z, w, s, los, observer_height=1.65, precision="mixed64") as eng:
         cm, tm, _ = eng.run()
     assert np.array_equal(bits(c64), bits(cm)) and np.array_equal(bits(t64), bits(tm))
+
+
+@pytest.mark.parametrize("angle", [0, 46])
+def test_shapes_7201(tvs, oracle, angle):
+    """The large-region geometry (7201^2, 2400-cell line of sight): 6791-point
+    windows of a 51.9 M-point sector order."""
+    w, s, los = 7201, 30.0, 72000
+    g = oracle.geometry(w, s, los)
+    d0, x0, f0 = oracle.compile_band_data(g, float(angle))
+    with tvs.Engine(np.zeros(w * w, np.float32), w, s, los) as eng:
+        d1, x1, f1 = eng.band_shape(angle)
+    assert f0 == f1 and np.array_equal(d0, d1) and np.array_equal(bits(x0), bits(x1))

@@ -118,6 +118,7 @@ SIGNATURES = {
     "tvs_read_rechecks": (_INT, [_VP, _P(_U64), _INT]),
     "tvs_stream": (_VP, [_VP]),
     "tvs_last_launch_count": (_U64, [_VP]),
+    "tvs_device_bytes": (_U64, [_VP]),
     "tvs_selftest_division": (_INT, [_I32, _U64, _U64, _P(_U64)]),
     "tvs_measure_fp32_issue": (_INT, [_I32, _P(ctypes.c_double)]),
     "tvs_compute_sector_noalloc": (_INT, [_P(Params), _VP, _U32, _VP, _VP, _VP]),
@@ -305,6 +306,9 @@ class Engine:
 
     def last_launch_count(self):
         return lib().tvs_last_launch_count(self.ctx)
+
+    def device_bytes(self):
+        return lib().tvs_device_bytes(self.ctx)
 
 
 def selftest_division(n, seed=0, device=0):

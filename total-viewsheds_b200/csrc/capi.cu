@@ -49,6 +49,7 @@ struct tvs_context {
     float *d_sf = nullptr, *d_sb = nullptr;
     // sectors whose shape stage ran since the last tvs_device_finish
     bool pending[tvs::kSectorSteps] = {};
+    uint64_t device_bytes = 0;  // everything this context allocated on the device
 };
 
 namespace {
@@ -273,6 +274,9 @@ int ensure_rings(tvs_context *c) {
     cudaError_t e = cudaMalloc(&c->d_rings, c->g.ring_slots_per_sector * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMalloc(&c->d_spill, (size_t)c->spill_cap * sizeof(uint4));
     if (e == cudaSuccess) e = cudaMalloc(&c->d_counters, 4 * sizeof(uint32_t));
+    if (e == cudaSuccess)
+        c->device_bytes += c->g.ring_slots_per_sector * sizeof(uint32_t) +
+                           (size_t)c->spill_cap * sizeof(uint4) + 4 * sizeof(uint32_t);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return fail(c, e == cudaErrorMemoryAllocation ? TVS_ERR_OUT_OF_MEMORY : TVS_ERR_CUDA,
@@ -286,6 +290,7 @@ int ensure_plain_scratch(tvs_context *c) {
     const uint64_t n = (uint64_t)(c->row_end - c->row_begin) * c->g.tvs_width;
     TVS_CUDA(c, cudaMalloc(&c->d_sf, std::max<uint64_t>(n, 1) * sizeof(float)));
     TVS_CUDA(c, cudaMalloc(&c->d_sb, std::max<uint64_t>(n, 1) * sizeof(float)));
+    c->device_bytes += 2 * std::max<uint64_t>(n, 1) * sizeof(float);
     return TVS_OK;
 }
 
@@ -548,11 +553,15 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
         {(void **)&c->d_deltas, (size_t)slots * bds * sizeof(int32_t)},
         {(void **)&c->d_dists, (size_t)slots * bds * sizeof(float)},
     };
-    for (auto &a : allocs)
+    for (auto &a : allocs) {
         if ((e = cudaMalloc(a.p, a.bytes)) != cudaSuccess) return bail(e, "cudaMalloc");
-    if (params->precision != TVS_PRECISION_EXACT32 &&
-        (e = cudaMalloc(&c->d_cum64, count * sizeof(double))) != cudaSuccess)
-        return bail(e, "cudaMalloc");
+        c->device_bytes += a.bytes;
+    }
+    if (params->precision != TVS_PRECISION_EXACT32) {
+        if ((e = cudaMalloc(&c->d_cum64, count * sizeof(double))) != cudaSuccess)
+            return bail(e, "cudaMalloc");
+        c->device_bytes += count * sizeof(double);
+    }
     // Per-sector trigonometry on the host (glibc, as Rust std on linux-gnu):
     // axes.rs:95 shifts the angle in f32, axes.rs:127 adds 90 in f32.
     std::vector<tvs::SectorTrig> trig(slots);
@@ -827,6 +836,8 @@ int tvs_read_rechecks(tvs_context *ctx, uint64_t *count, int reset) {
 void *tvs_stream(const tvs_context *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
 uint64_t tvs_last_launch_count(const tvs_context *ctx) { return ctx ? ctx->launches : 0; }
+
+uint64_t tvs_device_bytes(const tvs_context *ctx) { return ctx ? ctx->device_bytes : 0; }
 
 int tvs_run(tvs_context *ctx, float *cumulative_out, float *total_out, int want_rings,
             tvs_sector_callback callback, void *user) {

@@ -196,7 +196,7 @@ k_sweep_queue(QueueArgs a) {
                 s_boff[i] = (long long)go[i].x * (long long)sizeof(float);
                 if (kF64) {
                     s_dtab[i] = a.dtab[(uint64_t)slot * a.step_cap + i];
-                } else {
+                } else if (kPacked) {  // only the packed loop reserves these 32 B per step
                     PackedStep p;
                     p.y = pk(t.x, t.x);
                     p.nd = pk(-t.y, -t.y);
@@ -539,10 +539,11 @@ cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, cudaStream_t s
     const bool f64 = precision == TVS_PRECISION_FP64;
     if (!f64 && !mix && precision != TVS_PRECISION_EXACT32) return cudaErrorInvalidValue;
     if (mix && !a.hmax) return cudaErrorInvalidValue;
-    // ctl + {steps, byte offsets} + FP64 double tables or EXACT32 packed tables (32 B each)
-    const size_t smem = 32 + (size_t)a.step_cap * (sizeof(float4) + sizeof(long long) + 32);
     const PovShape sh = queue_shape();
     const bool packed = queue_packed();
+    // ctl + {steps, byte offsets} + FP64 double tables or packed exact-f32 tables (32 B each)
+    const bool wide = f64 || mix || packed;
+    const size_t smem = 32 + (size_t)a.step_cap * (sizeof(float4) + sizeof(long long) + (wide ? 32 : 0));
 #define TVS_Q(X, Y)                                                                    \
     if (sh.px == X && sh.py == Y)                                                      \
         return mix ? launch_queue_t<TVS_PRECISION_MIXED64, X, Y, false>(a, smem, s)    \
