@@ -196,6 +196,53 @@ uint64_t tvs_last_launch_count(const tvs_context *ctx);
  * added, the ring buffers on the first run that asks for ring records). */
 uint64_t tvs_device_bytes(const tvs_context *ctx);
 
+/* ---- sweep configuration and autotuning ------------------------------ */
+
+/* Points of view per thread of the persistent sweep: points_x columns 32
+ * apart times points_y rows 8 apart (1x1, 2x1, 4x1, 2x2, 8x1), i.e. a CTA tile
+ * of 32*points_x x 8*points_y points; packed != 0 selects the packed f32x2
+ * arithmetic (exact f32 only).  Results do not depend on it. */
+typedef struct tvs_sweep_config {
+    int32_t points_x;
+    int32_t points_y;
+    int32_t packed;
+} tvs_sweep_config;
+
+int tvs_set_sweep_config(tvs_context *ctx, const tvs_sweep_config *cfg);
+int tvs_get_sweep_config(const tvs_context *ctx, tvs_sweep_config *cfg);
+/* Times every candidate configuration on sectors [0, sample_sectors) of this
+ * context and keeps the fastest (returned in *chosen, nullable).  The device
+ * surfaces are undefined afterwards: reset before the next run. */
+int tvs_autotune(tvs_context *ctx, uint32_t sample_sectors, tvs_sweep_config *chosen);
+
+/* ---- batches of DEM tiles --------------------------------------------- */
+
+/* No counterpart in the reference (which runs one DEM per process).  Many DEM
+ * tiles of uneven, possibly rectangular size: every run computes all 180
+ * sectors of every tile with one shape launch and one persistent sweep,
+ * captured in a CUDA graph on the first run and replayed afterwards.
+ * params[i] and elevations[i] describe tile i (same device and precision for
+ * every tile). */
+typedef struct tvs_batch tvs_batch;
+
+int tvs_batch_create(const tvs_params *params, const float *const *elevations, uint32_t n_dems,
+                     tvs_batch **out);
+void tvs_batch_destroy(tvs_batch *batch);
+const char *tvs_batch_last_error(const tvs_batch *batch);
+uint32_t tvs_batch_size(const tvs_batch *batch);
+int tvs_batch_geometry(const tvs_batch *batch, uint32_t dem, tvs_geometry *out);
+int tvs_batch_set_sweep_config(tvs_batch *batch, const tvs_sweep_config *cfg);
+int tvs_batch_get_sweep_config(const tvs_batch *batch, tvs_sweep_config *cfg);
+/* As tvs_autotune, on the whole batch (drops the captured graph). */
+int tvs_batch_autotune(tvs_batch *batch, uint32_t sample_sectors, tvs_sweep_config *chosen);
+/* Enqueue one full run (graph replay) on the batch's stream. */
+int tvs_batch_run(tvs_batch *batch);
+/* Wait and report the first error of the last run. */
+int tvs_batch_finish(tvs_batch *batch);
+int tvs_batch_read(tvs_batch *batch, uint32_t dem, float *cumulative_out, float *total_out);
+void *tvs_batch_stream(const tvs_batch *batch);
+uint64_t tvs_batch_device_bytes(const tvs_batch *batch);
+
 /* ---- allocation-free form -------------------------------------------- */
 
 /* No counterpart in the reference.  One sector for callers that cannot

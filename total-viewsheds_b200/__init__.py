@@ -88,6 +88,14 @@ class SectorStats(ctypes.Structure):
     ]
 
 
+class SweepConfig(ctypes.Structure):
+    _fields_ = [("points_x", ctypes.c_int32), ("points_y", ctypes.c_int32),
+                ("packed", ctypes.c_int32)]
+
+    def __repr__(self):
+        return f"{self.points_x}x{self.points_y}{' packed' if self.packed else ''}"
+
+
 SECTOR_CALLBACK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32,
                                    ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint64,
                                    ctypes.POINTER(SectorStats))
@@ -122,6 +130,22 @@ SIGNATURES = {
     "tvs_selftest_division": (_INT, [_I32, _U64, _U64, _P(_U64)]),
     "tvs_measure_fp32_issue": (_INT, [_I32, _P(ctypes.c_double)]),
     "tvs_compute_sector_noalloc": (_INT, [_P(Params), _VP, _U32, _VP, _VP, _VP]),
+    "tvs_set_sweep_config": (_INT, [_VP, _P(SweepConfig)]),
+    "tvs_get_sweep_config": (_INT, [_VP, _P(SweepConfig)]),
+    "tvs_autotune": (_INT, [_VP, _U32, _P(SweepConfig)]),
+    "tvs_batch_create": (_INT, [_P(Params), _P(ctypes.c_void_p), _U32, _P(_VP)]),
+    "tvs_batch_destroy": (None, [_VP]),
+    "tvs_batch_last_error": (ctypes.c_char_p, [_VP]),
+    "tvs_batch_size": (_U32, [_VP]),
+    "tvs_batch_geometry": (_INT, [_VP, _U32, _P(Geometry)]),
+    "tvs_batch_set_sweep_config": (_INT, [_VP, _P(SweepConfig)]),
+    "tvs_batch_get_sweep_config": (_INT, [_VP, _P(SweepConfig)]),
+    "tvs_batch_autotune": (_INT, [_VP, _U32, _P(SweepConfig)]),
+    "tvs_batch_run": (_INT, [_VP]),
+    "tvs_batch_finish": (_INT, [_VP]),
+    "tvs_batch_read": (_INT, [_VP, _U32, _VP, _VP]),
+    "tvs_batch_stream": (_VP, [_VP]),
+    "tvs_batch_device_bytes": (_U64, [_VP]),
 }
 
 _lib = None
@@ -298,6 +322,21 @@ class Engine:
     def stream(self):
         return lib().tvs_stream(self.ctx)
 
+    def sweep_config(self):
+        c = SweepConfig()
+        self._check(lib().tvs_get_sweep_config(self.ctx, ctypes.byref(c)))
+        return c
+
+    def set_sweep_config(self, points_x, points_y, packed=False):
+        c = SweepConfig(points_x, points_y, 1 if packed else 0)
+        self._check(lib().tvs_set_sweep_config(self.ctx, ctypes.byref(c)))
+
+    def autotune(self, sample_sectors=4):
+        """Time the sweep configurations on a few sectors and keep the fastest."""
+        c = SweepConfig()
+        self._check(lib().tvs_autotune(self.ctx, sample_sectors, ctypes.byref(c)))
+        return c
+
     def read_rechecks(self, reset=True):
         """MIXED64: comparisons re-decided in FP64 since the last reset."""
         v = ctypes.c_uint64()
@@ -309,6 +348,85 @@ class Engine:
 
     def device_bytes(self):
         return lib().tvs_device_bytes(self.ctx)
+
+
+class Batch:
+    """Many DEM tiles (uneven, possibly rectangular), all 180 sectors each, one
+    shape launch and one persistent sweep per run (a replayed CUDA graph)."""
+
+    def __init__(self, dems, **kw):
+        """dems: list of (heights [H, W] f32, scale, max_line_of_sight)."""
+        self.params = (Params * len(dems))()
+        self._heights = []
+        for i, (z, scale, los) in enumerate(dems):
+            z = np.ascontiguousarray(z, np.float32)
+            h, w = z.shape
+            self.params[i] = make_params(w, scale, los, height=h, **kw)
+            self._heights.append(z)
+        ptrs = (ctypes.c_void_p * len(dems))(*[_ptr(z).value for z in self._heights])
+        b = ctypes.c_void_p()
+        rc = lib().tvs_batch_create(self.params, ptrs, len(dems), ctypes.byref(b))
+        if rc:
+            _raise(rc)
+        self.b = b
+        self.geometry = []
+        for i in range(len(dems)):
+            g = Geometry()
+            lib().tvs_batch_geometry(self.b, i, ctypes.byref(g))
+            self.geometry.append(g)
+
+    def _check(self, rc):
+        if rc:
+            msg = lib().tvs_batch_last_error(self.b)
+            raise TvsError(rc, msg.decode() if msg else "error")
+
+    def close(self):
+        if getattr(self, "b", None):
+            lib().tvs_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __len__(self):
+        return lib().tvs_batch_size(self.b)
+
+    def autotune(self, sample_sectors=4):
+        c = SweepConfig()
+        self._check(lib().tvs_batch_autotune(self.b, sample_sectors, ctypes.byref(c)))
+        return c
+
+    def set_sweep_config(self, points_x, points_y, packed=False):
+        c = SweepConfig(points_x, points_y, 1 if packed else 0)
+        self._check(lib().tvs_batch_set_sweep_config(self.b, ctypes.byref(c)))
+
+    def run(self):
+        self._check(lib().tvs_batch_run(self.b))
+
+    def finish(self):
+        self._check(lib().tvs_batch_finish(self.b))
+
+    def read(self, dem):
+        n = self.geometry[dem].computable_points_count
+        cum = np.empty(n, np.float32)
+        total = np.empty(n, np.float32)
+        self._check(lib().tvs_batch_read(self.b, dem, _ptr(cum), _ptr(total)))
+        return cum, total
+
+    def stream(self):
+        return lib().tvs_batch_stream(self.b)
+
+    def device_bytes(self):
+        return lib().tvs_batch_device_bytes(self.b)
 
 
 def selftest_division(n, seed=0, device=0):

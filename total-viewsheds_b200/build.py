@@ -19,7 +19,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libtvs_cuda.so"
 CLI = PKG / "tvs"
-SOURCES = ["capi.cu", "shape.cu", "sweep.cu", "sweep_queue.cu", "noalloc.cu"]
+SOURCES = ["capi.cu", "shape.cu", "sweep.cu", "sweep_queue.cu", "noalloc.cu", "batch.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

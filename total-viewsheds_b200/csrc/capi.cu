@@ -12,45 +12,7 @@
 #include "tvs.h"
 #include "tvs_internal.cuh"
 
-struct tvs_context {
-    tvs_params p{};
-    tvs_geometry g{};
-    uint32_t row_begin = 0, row_end = 0;
-    int64_t pov_min = 0, pov_max = 0;
-    uint32_t step_cap = 0;
-    cudaStream_t stream = nullptr;
-    std::string err;
-    uint64_t launches = 0;
-
-    float *d_elev = nullptr;
-    float *d_cum = nullptr;
-    float *d_total = nullptr;
-    double *d_cum64 = nullptr;
-    tvs::SectorTrig *d_trig = nullptr;
-    tvs::ShapeHeader *d_hdr = nullptr;   // [180 + 1]: the last slot serves tvs_axes
-    float4 *d_steps = nullptr;
-    int2 *d_offs = nullptr;
-    double4 *d_dtab = nullptr;
-    // persistent-sweep work queue
-    uint32_t *d_queue = nullptr;
-    uint32_t *d_done = nullptr;
-    uint32_t done_cap = 0;
-    int32_t *d_error = nullptr;
-    float *d_hmax = nullptr;  // max |elevation| + |observer height| (MIXED64 window)
-    unsigned long long *d_rechecks = nullptr;  // MIXED64 FP64 re-decisions
-    int32_t *d_deltas = nullptr;
-    float *d_dists = nullptr;
-    // ring output (allocated on first use)
-    uint32_t *d_rings = nullptr;
-    uint4 *d_spill = nullptr;
-    uint32_t *d_counters = nullptr;
-    uint32_t spill_cap = 0;
-    // plain-kernel scratch (allocated on first use)
-    float *d_sf = nullptr, *d_sb = nullptr;
-    // sectors whose shape stage ran since the last tvs_device_finish
-    bool pending[tvs::kSectorSteps] = {};
-    uint64_t device_bytes = 0;  // everything this context allocated on the device
-};
+#include "tvs_context.hpp"
 
 namespace {
 
@@ -170,7 +132,7 @@ int derive_geometry(const tvs_params *p, tvs_geometry *g, std::string *msg) {
 void free_all(tvs_context *c) {
     void *ptrs[] = {c->d_elev, c->d_cum, c->d_total, c->d_cum64, c->d_trig, c->d_hdr,
                     c->d_steps, c->d_offs, c->d_dtab, c->d_queue, c->d_done, c->d_error, c->d_hmax,
-                    c->d_rechecks,
+                    c->d_rechecks, c->d_qdem,
                     c->d_deltas, c->d_dists, c->d_rings, c->d_spill, c->d_counters, c->d_sf,
                     c->d_sb};
     for (void *p : ptrs)
@@ -302,6 +264,40 @@ int enqueue_shape(tvs_context *c, uint32_t first, uint32_t count) {
     return TVS_OK;
 }
 
+// This context as the one-DEM descriptor of the queue sweep, tiled for the
+// context's configuration (uploaded again only when the configuration changes).
+tvs::QueueDem queue_dem(const tvs_context *c) {
+    tvs::QueueDem d{};
+    d.elev = c->d_elev;
+    d.width = c->g.width;
+    d.tvs_width = c->g.tvs_width;
+    d.los = c->g.max_los_as_points;
+    d.row_begin = c->row_begin;
+    d.row_end = c->row_end;
+    d.observer_height = c->p.observer_height;
+    d.step_cap = c->step_cap;
+    d.hdr = c->d_hdr;
+    d.steps = c->d_steps;
+    d.offs = c->d_offs;
+    d.dtab = c->d_dtab;
+    d.cumulative = c->d_cum;
+    d.total = c->d_total;
+    d.cumulative64 = c->d_cum64;
+    d.hmax = c->d_hmax;
+    return d;
+}
+
+int upload_queue_dem(tvs_context *c) {
+    const tvs::QueueConfig &q = c->qcfg, &u = c->qcfg_uploaded;
+    if (q.px == u.px && q.py == u.py && q.packed == u.packed) return TVS_OK;
+    tvs::QueueDem d = queue_dem(c);
+    uint32_t done_total = 0;
+    tvs::queue_tile(&d, 1, q, &c->q_tiles_per_sector, &done_total);
+    TVS_CUDA(c, cudaMemcpyAsync(c->d_qdem, &d, sizeof d, cudaMemcpyHostToDevice, c->stream));
+    c->qcfg_uploaded = q;
+    return TVS_OK;
+}
+
 // Sweep sectors [first, first+count) (slots == angles).  With rings, count is 1.
 int enqueue_sweep(tvs_context *c, uint32_t first, uint32_t count, bool rings) {
     if (c->p.sweep_kernel == TVS_SWEEP_PLAIN) {
@@ -343,32 +339,23 @@ int enqueue_sweep(tvs_context *c, uint32_t first, uint32_t count, bool rings) {
         c->g.band_steps_filled + std::min(c->g.band_deltas_size - c->g.band_steps_filled, 2u);
     const SweepImpl impl = sweep_impl();
     if (!rings && impl == SweepImpl::Queue) {
+        int rc = upload_queue_dem(c);
+        if (rc) return rc;
         tvs::QueueArgs q{};
-        q.elev = c->d_elev;
-        q.width = c->g.width;
-        q.tvs_width = c->g.tvs_width;
-        q.los = c->g.max_los_as_points;
-        q.row_begin = c->row_begin;
-        q.row_end = c->row_end;
-        q.observer_height = c->p.observer_height;
+        q.dems = c->d_qdem;
+        q.n_dems = 1;
         q.first_sector = first;
         q.n_sectors = count;
-        q.step_cap = c->step_cap;
-        q.hdr = c->d_hdr;
-        q.steps = c->d_steps;
-        q.offs = c->d_offs;
-        q.dtab = c->d_dtab;
-        q.cumulative = c->d_cum;
-        q.total = c->d_total;
-        q.cumulative64 = c->d_cum64;
+        q.tiles_per_sector = c->q_tiles_per_sector;
+        q.max_step_cap = c->step_cap;
         q.queue = c->d_queue;
         q.done = c->d_done;
+        q.done_total = c->q_tiles_per_sector;
         q.done_cap = c->done_cap;
         q.error = c->d_error;
-        q.hmax = c->d_hmax;
-        q.rechecks = c->d_rechecks;
         q.spin_limit = 1u << 23;  // ~2-4 s of 256 ns sleeps; a real wait is one item (~1 ms)
-        TVS_CUDA(c, tvs::launch_sweep_queue(q, (int)c->p.precision, c->stream));
+        q.rechecks = c->d_rechecks;
+        TVS_CUDA(c, tvs::launch_sweep_queue(q, (int)c->p.precision, c->qcfg, c->stream));
         c->launches++;
         return TVS_OK;
     }
@@ -468,6 +455,14 @@ int collect_rings(tvs_context *c, uint32_t *rings, uint64_t rings_len, tvs_secto
 // no context).
 void tvs_set_create_error(const std::string &msg) { g_create_error = msg; }
 
+namespace tvs_host {
+tvs::ShapeArgs shape_args_of(tvs_context *c, uint32_t first_slot) { return shape_args(c, first_slot); }
+tvs::QueueDem queue_dem_of(const tvs_context *c) { return queue_dem(c); }
+int header_status_of(tvs_context *c, uint32_t first, uint32_t count) {
+    return header_status(c, first, count);
+}
+}  // namespace tvs_host
+
 extern "C" {
 
 int tvs_abi_version(void) { return TVS_ABI_VERSION; }
@@ -521,6 +516,7 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
     }
     c->step_cap = (g.band_steps_filled + 2 + 3) & ~3u;
     c->done_cap = tvs::queue_tiles_bound(g.tvs_width, re - rb);
+    c->qcfg = tvs::default_queue_config();
     auto bail = [&](cudaError_t e, const char *what) {
         std::string m = std::string(what) + ": " + cudaGetErrorString(e);
         int code = e == cudaErrorMemoryAllocation ? TVS_ERR_OUT_OF_MEMORY : TVS_ERR_CUDA;
@@ -550,6 +546,7 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
         {(void **)&c->d_error, sizeof(int32_t)},
         {(void **)&c->d_hmax, sizeof(float)},
         {(void **)&c->d_rechecks, sizeof(unsigned long long)},
+        {(void **)&c->d_qdem, sizeof(tvs::QueueDem)},
         {(void **)&c->d_deltas, (size_t)slots * bds * sizeof(int32_t)},
         {(void **)&c->d_dists, (size_t)slots * bds * sizeof(float)},
     };
@@ -821,6 +818,64 @@ int tvs_read_surfaces(tvs_context *ctx, float *cumulative_out, float *total_out)
 }
 
 const float *tvs_device_cumulative(const tvs_context *ctx) { return ctx ? ctx->d_cum : nullptr; }
+
+int tvs_set_sweep_config(tvs_context *ctx, const tvs_sweep_config *cfg) {
+    if (!ctx || !cfg) return TVS_ERR_INVALID_ARGUMENT;
+    tvs::QueueConfig c{cfg->points_x, cfg->points_y, cfg->packed != 0};
+    if (!tvs::queue_config_valid(c))
+        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "unsupported points-per-thread shape");
+    ctx->qcfg = c;
+    return TVS_OK;
+}
+
+int tvs_get_sweep_config(const tvs_context *ctx, tvs_sweep_config *cfg) {
+    if (!ctx || !cfg) return TVS_ERR_INVALID_ARGUMENT;
+    cfg->points_x = ctx->qcfg.px;
+    cfg->points_y = ctx->qcfg.py;
+    cfg->packed = ctx->qcfg.packed;
+    return TVS_OK;
+}
+
+int tvs_autotune(tvs_context *ctx, uint32_t sample_sectors, tvs_sweep_config *chosen) {
+    if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
+    if (sample_sectors == 0 || sample_sectors > tvs::kSectorSteps)
+        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "sample_sectors must be in [1, 180]");
+    TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
+    const bool exact = ctx->p.precision == TVS_PRECISION_EXACT32;
+    const tvs::QueueConfig cands[] = {{1, 1, 0}, {2, 1, 0}, {4, 1, 0}, {2, 2, 0},
+                                      {2, 1, 1}, {4, 1, 1}};
+    cudaEvent_t t0, t1;
+    TVS_CUDA(ctx, cudaEventCreate(&t0));
+    TVS_CUDA(ctx, cudaEventCreate(&t1));
+    float best = 1e30f;
+    tvs::QueueConfig best_cfg = ctx->qcfg;
+    int rc = enqueue_shape(ctx, 0, sample_sectors);
+    for (const tvs::QueueConfig &c : cands) {
+        if (rc) break;
+        if (c.packed && !exact) continue;
+        ctx->qcfg = c;
+        float ms = 0.0f;
+        for (int rep = 0; rep < 2 && rc == TVS_OK; rep++) {  // the first run warms up
+            cudaEventRecord(t0, ctx->stream);
+            rc = enqueue_sweep(ctx, 0, sample_sectors, false);
+            cudaEventRecord(t1, ctx->stream);
+            if (rc == TVS_OK && cudaEventSynchronize(t1) != cudaSuccess)
+                rc = fail(ctx, TVS_ERR_CUDA, "autotune run failed");
+            if (rc == TVS_OK) cudaEventElapsedTime(&ms, t0, t1);
+        }
+        if (rc == TVS_OK && ms < best) {
+            best = ms;
+            best_cfg = c;
+        }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    ctx->qcfg = best_cfg;
+    for (bool &p : ctx->pending) p = false;
+    if (rc) return rc;
+    if (chosen) tvs_get_sweep_config(ctx, chosen);
+    return TVS_OK;
+}
 
 int tvs_read_rechecks(tvs_context *ctx, uint64_t *count, int reset) {
     if (!ctx || !count) return TVS_ERR_INVALID_ARGUMENT;

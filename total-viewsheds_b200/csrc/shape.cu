@@ -140,14 +140,15 @@ struct ShapeSmem {
 
 }  // namespace
 
-__global__ void __launch_bounds__(kShapeThreads, 1)
-k_shape(ShapeArgs a, uint64_t rank_lo, uint64_t rank_count, int axes_mode) {
+// One sector of one DEM (the whole CTA).
+__device__ __forceinline__ void shape_sector(const ShapeArgs &a, const uint32_t sector,
+                                             const uint64_t rank_lo, const uint64_t rank_count,
+                                             const int axes_mode) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ShapeSmem &sm = *reinterpret_cast<ShapeSmem *>(smem_raw);
     unsigned long long *cand = reinterpret_cast<unsigned long long *>(smem_raw + sizeof(ShapeSmem));
     unsigned long long *win = cand + kCandidateCap;
 
-    const uint32_t sector = blockIdx.x;
     const SectorTrig tr = a.trig[sector];
     const uint32_t W = a.width, H = a.height;
     const uint64_t rank_hi = rank_lo + rank_count - 1;
@@ -319,6 +320,18 @@ k_shape(ShapeArgs a, uint64_t rank_lo, uint64_t rank_count, int axes_mode) {
     }
 }
 
+__global__ void __launch_bounds__(kShapeThreads, 1)
+k_shape(ShapeArgs a, uint64_t rank_lo, uint64_t rank_count, int axes_mode) {
+    shape_sector(a, blockIdx.x, rank_lo, rank_count, axes_mode);
+}
+
+// Many DEMs at once: CTA b handles sector b % n_sectors of DEM b / n_sectors.
+__global__ void __launch_bounds__(kShapeThreads, 1)
+k_shape_batch(const ShapeArgs *args, uint32_t n_sectors) {
+    const ShapeArgs a = args[blockIdx.x / n_sectors];
+    shape_sector(a, blockIdx.x % n_sectors, a.size / 2 - a.band_samples / 2, a.band_samples, 0);
+}
+
 // axes.rs:154-189: the f32 sight distance of every point.
 __global__ void k_sight_distances(SectorTrig t, uint32_t W, uint32_t H, float *out) {
     const uint64_t n = (uint64_t)W * H;
@@ -358,6 +371,21 @@ cudaError_t launch_shape(const ShapeArgs &a, uint32_t n_sectors, cudaStream_t s)
         rank_count = a.band_samples;
     }
     k_shape<<<n_sectors, kShapeThreads, smem, s>>>(a, rank_lo, rank_count, axes_mode);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_shape_batch(const ShapeArgs *d_args, uint32_t n_dems, uint32_t n_sectors,
+                               cudaStream_t s) {
+    static bool configured = false;
+    const size_t smem = shape_smem_bytes();
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(k_shape_batch,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    if (n_dems == 0 || n_sectors == 0) return cudaSuccess;
+    k_shape_batch<<<n_dems * n_sectors, kShapeThreads, smem, s>>>(d_args, n_sectors);
     return cudaGetLastError();
 }
 

@@ -92,12 +92,16 @@ struct PackedStep {
 };
 
 struct QueueCtl {
+    QueueDem dem;           // the current item's DEM (copied from the descriptor array)
     uint32_t item;
+    uint32_t dem_index;     // descriptor index of `dem`
+    uint32_t sector;        // the staged sector
+    uint32_t tile;          // the current item's tile within its DEM
     int32_t sector_status;  // the staged sector's shape status
     int32_t wait_status;    // this item's dependency wait
     uint32_t n_steps;
     uint32_t n_fast;
-    uint32_t pad[3];
+    bool restage;
 };
 
 // Per-point state of one direction.
@@ -161,27 +165,47 @@ k_sweep_queue(QueueArgs a) {
     QueueCtl &ctl = *reinterpret_cast<QueueCtl *>(smem);
     float4 *s_steps = reinterpret_cast<float4 *>(smem + sizeof(QueueCtl));
     // forward DEM-id offset of each step, in bytes (a 64-bit add per base address)
-    long long *s_boff = reinterpret_cast<long long *>(s_steps + a.step_cap);
-    double4 *s_dtab = reinterpret_cast<double4 *>(s_boff + a.step_cap);  // FP64 only
-    PackedStep *s_pk = reinterpret_cast<PackedStep *>(s_boff + a.step_cap);  // EXACT32 only
+    long long *s_boff = reinterpret_cast<long long *>(s_steps + a.max_step_cap);
+    double4 *s_dtab = reinterpret_cast<double4 *>(s_boff + a.max_step_cap);  // FP64 only
+    PackedStep *s_pk = reinterpret_cast<PackedStep *>(s_boff + a.max_step_cap);  // packed only
     const uint32_t tid = threadIdx.y * kTileX + threadIdx.x;
-    const uint32_t n_tiles = a.tiles_x * a.tiles_y;
-    const uint32_t n_items = n_tiles * a.n_sectors;
-    uint32_t cur = 0xFFFFFFFFu;
+    const uint32_t n_items = a.tiles_per_sector * a.n_sectors;
+    if (tid == 0) {
+        ctl.dem_index = 0xFFFFFFFFu;
+        ctl.sector = 0xFFFFFFFFu;
+    }
 
     for (;;) {
-        if (tid == 0) ctl.item = atomicAdd(a.queue, 1u);
+        if (tid == 0) {
+            const uint32_t item = atomicAdd(a.queue, 1u);
+            ctl.item = item;
+            if (item < n_items) {
+                const uint32_t s = item / a.tiles_per_sector;
+                const uint32_t r = item - s * a.tiles_per_sector;
+                // the DEM whose tiles hold r (tile_base ascends)
+                uint32_t lo = 0, hi = a.n_dems - 1;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi + 1) >> 1;
+                    if (a.dems[mid].tile_base <= r) lo = mid; else hi = mid - 1;
+                }
+                ctl.restage = lo != ctl.dem_index || s != ctl.sector;
+                if (lo != ctl.dem_index) ctl.dem = a.dems[lo];
+                ctl.dem_index = lo;
+                ctl.sector = s;
+                ctl.tile = r - ctl.dem.tile_base;
+            }
+        }
         __syncthreads();
-        const uint32_t item = ctl.item;
-        if (item >= n_items) break;
-        const uint32_t s = item / n_tiles, tile = item - s * n_tiles;
-        if (s != cur) {  // stage this sector's tables
+        if (ctl.item >= n_items) break;
+        const QueueDem &D = ctl.dem;
+        const uint32_t s = ctl.sector, tile = ctl.tile;
+        if (ctl.restage) {  // stage this DEM's sector tables
             const uint32_t slot = a.first_sector + s;
-            const ShapeHeader *h = a.hdr + slot;
+            const ShapeHeader *h = D.hdr + slot;
             const uint32_t n = h->n_steps;
-            const float4 *gs = a.steps + (uint64_t)slot * a.step_cap;
-            const int2 *go = a.offs + (uint64_t)slot * a.step_cap;
-            const float hmax = kMix ? *a.hmax : 0.0f;
+            const float4 *gs = D.steps + (uint64_t)slot * D.step_cap;
+            const int2 *go = D.offs + (uint64_t)slot * D.step_cap;
+            const float hmax = kMix ? *D.hmax : 0.0f;
             for (uint32_t i = tid; i < n; i += kThreads) {
                 const float4 t = gs[i];
                 s_steps[i] = t;
@@ -195,7 +219,7 @@ k_sweep_queue(QueueArgs a) {
                 }
                 s_boff[i] = (long long)go[i].x * (long long)sizeof(float);
                 if (kF64) {
-                    s_dtab[i] = a.dtab[(uint64_t)slot * a.step_cap + i];
+                    s_dtab[i] = D.dtab[(uint64_t)slot * D.step_cap + i];
                 } else if (kPacked) {  // only the packed loop reserves these 32 B per step
                     PackedStep p;
                     p.y = pk(t.x, t.x);
@@ -210,13 +234,12 @@ k_sweep_queue(QueueArgs a) {
                 ctl.n_steps = n;
                 ctl.n_fast = h->n_fast;
             }
-            cur = s;
         }
         // This tile's previous sector must be complete (bounded wait).
         if (tid == 0) {
             ctl.wait_status = TVS_OK;
             if (s > 0) {
-                const volatile uint32_t *d = a.done + tile;
+                const volatile uint32_t *d = a.done + D.done_base + tile;
                 const volatile int32_t *err = a.error;
                 uint32_t spins = 0;
                 while (*d < s) {
@@ -234,9 +257,9 @@ k_sweep_queue(QueueArgs a) {
         __syncthreads();
         const bool run = ctl.sector_status == TVS_OK && ctl.wait_status == TVS_OK;
         const uint32_t n = ctl.n_steps, n_fast = ctl.n_fast;
-        const uint32_t bx = tile % a.tiles_x, by = tile / a.tiles_x;
+        const uint32_t bx = tile % D.tiles_x, by = tile / D.tiles_x;
         const uint32_t tx0 = bx * (kTileX * kPx) + threadIdx.x;
-        const uint32_t ty0 = a.row_begin + by * (kTileY * kPy) + threadIdx.y;
+        const uint32_t ty0 = D.row_begin + by * (kTileY * kPy) + threadIdx.y;
         if (run) {
             const float *ep[kPy];
             using HP = typename std::conditional<kF64, double, float>::type;
@@ -247,14 +270,14 @@ k_sweep_queue(QueueArgs a) {
             for (int py = 0; py < kPy; py++) {
                 // rows past the grid are clamped, columns past it read padding;
                 // both are discarded
-                const uint32_t ty = min(ty0 + py * kTileY, a.row_end - 1);
-                ep[py] = a.elev + (int64_t)(ty + a.los) * a.width + tx0 + a.los;
+                const uint32_t ty = min(ty0 + py * kTileY, D.row_end - 1);
+                ep[py] = D.elev + (int64_t)(ty + D.los) * D.width + tx0 + D.los;
 #pragma unroll
                 for (int px = 0; px < kPx; px++) {
                     const float h0 = __ldg(ep[py] + kTileX * px);
-                    if (kF64) hp[py][px] = (HP)__dadd_rn((double)h0, (double)a.observer_height);
-                    else hp[py][px] = (HP)__fadd_rn(h0, a.observer_height);  // kernel.rs:134
-                    hp32[py][px] = __fadd_rn(h0, a.observer_height);
+                    if (kF64) hp[py][px] = (HP)__dadd_rn((double)h0, (double)D.observer_height);
+                    else hp[py][px] = (HP)__fadd_rn(h0, D.observer_height);  // kernel.rs:134
+                    hp32[py][px] = __fadd_rn(h0, D.observer_height);
                     cf[py][px].init();
                     cb[py][px].init();
                 }
@@ -437,64 +460,38 @@ k_sweep_queue(QueueArgs a) {
 #pragma unroll
             for (int py = 0; py < kPy; py++) {
                 const uint32_t ty = ty0 + py * kTileY;
-                if (ty >= a.row_end) continue;
+                if (ty >= D.row_end) continue;
 #pragma unroll
                 for (int px = 0; px < kPx; px++) {
                     const uint32_t tx = tx0 + kTileX * px;
-                    if (tx >= a.tvs_width) continue;
-                    const uint64_t p = (uint64_t)ty * a.tvs_width + tx;
+                    if (tx >= D.tvs_width) continue;
+                    const uint64_t p = (uint64_t)ty * D.tvs_width + tx;
                     // surfaces are read and written in L2 (another SM wrote the
                     // previous sector's values)
                     if constexpr (kF64) {
                         const double cum =
-                            __dadd_rn(__dadd_rn(__ldcg(a.cumulative64 + p), cf[py][px].s), cb[py][px].s);
-                        __stcg(a.cumulative64 + p, cum);
+                            __dadd_rn(__dadd_rn(__ldcg(D.cumulative64 + p), cf[py][px].s), cb[py][px].s);
+                        __stcg(D.cumulative64 + p, cum);
                         const float c32 = __double2float_rn(cum);
-                        __stcg(a.cumulative + p, c32);
-                        if (a.total) __stcg(a.total + p, __fadd_rn(__ldcg(a.total + p), c32));
+                        __stcg(D.cumulative + p, c32);
+                        if (D.total) __stcg(D.total + p, __fadd_rn(__ldcg(D.total + p), c32));
                     } else {
                         const float cum =
-                            __fadd_rn(__fadd_rn(__ldcg(a.cumulative + p), cf[py][px].s), cb[py][px].s);
-                        __stcg(a.cumulative + p, cum);                                  // kernel.rs:254
-                        if (a.total) __stcg(a.total + p, __fadd_rn(__ldcg(a.total + p), cum));  // compute.rs:206-214
+                            __fadd_rn(__fadd_rn(__ldcg(D.cumulative + p), cf[py][px].s), cb[py][px].s);
+                        __stcg(D.cumulative + p, cum);                                  // kernel.rs:254
+                        if (D.total) __stcg(D.total + p, __fadd_rn(__ldcg(D.total + p), cum));  // compute.rs:206-214
                     }
                 }
             }
         }
         __threadfence();   // this thread's surface writes before the tile's counter
         __syncthreads();
-        if (tid == 0) atomicAdd(a.done + tile, 1u);
+        if (tid == 0) atomicAdd(a.done + D.done_base + tile, 1u);
     }
 }
 
-struct PovShape { int px, py; };
-
-PovShape queue_shape() {
-    static PovShape v = [] {
-        const char *e = getenv("TVS_SWEEP_SHAPE");
-        PovShape d{2, 1};
-        if (!e) return d;
-        int x = 0, y = 0;
-        if (sscanf(e, "%dx%d", &x, &y) != 2) return d;
-        const PovShape ok[] = {{1, 1}, {2, 1}, {4, 1}, {2, 2}, {8, 1}};
-        for (const PovShape &k : ok)
-            if (k.px == x && k.py == y) return k;
-        return d;
-    }();
-    return v;
-}
-
-// Packed f32x2 fast loop (1) or scalar (0): TVS_SWEEP_PACKED overrides the default.
-bool queue_packed() {
-    static bool v = [] {
-        const char *e = getenv("TVS_SWEEP_PACKED");
-        return e ? atoi(e) != 0 : false;
-    }();
-    return v;
-}
-
 template <int kPrec, int kPx, int kPy, bool kPacked>
-cudaError_t launch_queue_t(const QueueArgs &a0, size_t smem, cudaStream_t s) {
+cudaError_t launch_queue_t(const QueueArgs &a, size_t smem, cudaStream_t s) {
     auto fn = k_sweep_queue<kPrec, kPx, kPy, kPacked>;
     static int blocks_per_sm = -1;
     static size_t configured_smem = 0;
@@ -510,16 +507,11 @@ cudaError_t launch_queue_t(const QueueArgs &a0, size_t smem, cudaStream_t s) {
         if (blocks_per_sm < 1) blocks_per_sm = 1;
         configured_smem = smem;
     }
-    QueueArgs a = a0;
-    const uint32_t rows = a.row_end - a.row_begin;
-    a.tiles_x = (a.tvs_width + kTileX * kPx - 1) / (kTileX * kPx);
-    a.tiles_y = (rows + kTileY * kPy - 1) / (kTileY * kPy);
-    const uint64_t tiles = (uint64_t)a.tiles_x * a.tiles_y;
-    if (tiles > a.done_cap) return cudaErrorInvalidValue;
+    if (a.done_total > a.done_cap) return cudaErrorInvalidValue;
     e = cudaMemsetAsync(a.queue, 0, sizeof(uint32_t), s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(a.done, 0, tiles * sizeof(uint32_t), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(a.done, 0, (size_t)a.done_total * sizeof(uint32_t), s);
     if (e != cudaSuccess) return e;
-    const uint64_t items = tiles * a.n_sectors;
+    const uint64_t items = (uint64_t)a.tiles_per_sector * a.n_sectors;
     const uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)blocks_per_sm * sms, items);
     fn<<<grid, dim3(kTileX, kTileY), smem, s>>>(a);
     return cudaGetLastError();
@@ -532,20 +524,59 @@ uint32_t queue_tiles_bound(uint32_t tvs_width, uint32_t rows) {
     return ((tvs_width + kTileX - 1) / kTileX) * ((rows + kTileY - 1) / kTileY);
 }
 
-cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, cudaStream_t s) {
-    const uint32_t rows = a.row_end - a.row_begin;
-    if (rows == 0 || a.tvs_width == 0 || a.n_sectors == 0) return cudaSuccess;
+bool queue_config_valid(const QueueConfig &c) {
+    const int ok[][2] = {{1, 1}, {2, 1}, {4, 1}, {2, 2}, {8, 1}};
+    for (const auto &k : ok)
+        if (k[0] == c.px && k[1] == c.py) return true;
+    return false;
+}
+
+QueueConfig default_queue_config() {
+    static QueueConfig v = [] {
+        QueueConfig d{2, 1, 0};
+        const char *e = getenv("TVS_SWEEP_SHAPE");
+        int x = 0, y = 0;
+        if (e && sscanf(e, "%dx%d", &x, &y) == 2) {
+            QueueConfig c{x, y, 0};
+            if (queue_config_valid(c)) d.px = x, d.py = y;
+        }
+        const char *p = getenv("TVS_SWEEP_PACKED");
+        if (p) d.packed = atoi(p) != 0;
+        return d;
+    }();
+    return v;
+}
+
+void queue_tile(QueueDem *dems, uint32_t n_dems, const QueueConfig &c, uint32_t *tiles_per_sector,
+                uint32_t *done_total) {
+    uint32_t base = 0;
+    for (uint32_t i = 0; i < n_dems; i++) {
+        QueueDem &d = dems[i];
+        const uint32_t rows = d.row_end - d.row_begin;
+        d.tiles_x = (d.tvs_width + kTileX * c.px - 1) / (kTileX * c.px);
+        d.tiles_y = (rows + kTileY * c.py - 1) / (kTileY * c.py);
+        d.tile_base = base;
+        d.done_base = base;
+        base += d.tiles_x * d.tiles_y;
+    }
+    *tiles_per_sector = base;
+    *done_total = base;
+}
+
+cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, const QueueConfig &c,
+                               cudaStream_t s) {
+    if (a.n_dems == 0 || a.tiles_per_sector == 0 || a.n_sectors == 0) return cudaSuccess;
     const bool mix = precision == TVS_PRECISION_MIXED64;
     const bool f64 = precision == TVS_PRECISION_FP64;
     if (!f64 && !mix && precision != TVS_PRECISION_EXACT32) return cudaErrorInvalidValue;
-    if (mix && !a.hmax) return cudaErrorInvalidValue;
-    const PovShape sh = queue_shape();
-    const bool packed = queue_packed();
+    if (!queue_config_valid(c)) return cudaErrorInvalidValue;
+    const bool packed = c.packed && !f64 && !mix;
     // ctl + {steps, byte offsets} + FP64 double tables or packed exact-f32 tables (32 B each)
     const bool wide = f64 || mix || packed;
-    const size_t smem = 32 + (size_t)a.step_cap * (sizeof(float4) + sizeof(long long) + (wide ? 32 : 0));
+    const size_t smem = sizeof(QueueCtl) +
+                        (size_t)a.max_step_cap * (sizeof(float4) + sizeof(long long) + (wide ? 32 : 0));
 #define TVS_Q(X, Y)                                                                    \
-    if (sh.px == X && sh.py == Y)                                                      \
+    if (c.px == X && c.py == Y)                                                        \
         return mix ? launch_queue_t<TVS_PRECISION_MIXED64, X, Y, false>(a, smem, s)    \
                : f64 ? launch_queue_t<TVS_PRECISION_FP64, X, Y, false>(a, smem, s)     \
                : packed ? launch_queue_t<TVS_PRECISION_EXACT32, X, Y, true>(a, smem, s) \

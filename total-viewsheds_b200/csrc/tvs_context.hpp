@@ -1,0 +1,60 @@
+// tvs_context.hpp -- the per-DEM context behind the C ABI (internal to the library).
+#pragma once
+
+#include <cstdint>
+#include <string>
+
+#include "tvs.h"
+#include "tvs_internal.cuh"
+
+struct tvs_context {
+    tvs_params p{};
+    tvs_geometry g{};
+    uint32_t row_begin = 0, row_end = 0;
+    int64_t pov_min = 0, pov_max = 0;
+    uint32_t step_cap = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    uint64_t launches = 0;
+
+    float *d_elev = nullptr;
+    float *d_cum = nullptr;
+    float *d_total = nullptr;
+    double *d_cum64 = nullptr;
+    tvs::SectorTrig *d_trig = nullptr;
+    tvs::ShapeHeader *d_hdr = nullptr;   // [180 + 1]: the last slot serves tvs_axes
+    float4 *d_steps = nullptr;
+    int2 *d_offs = nullptr;
+    double4 *d_dtab = nullptr;
+    // persistent-sweep work queue
+    uint32_t *d_queue = nullptr;
+    uint32_t *d_done = nullptr;
+    uint32_t done_cap = 0;
+    int32_t *d_error = nullptr;
+    float *d_hmax = nullptr;  // max |elevation| + |observer height| (MIXED64 window)
+    unsigned long long *d_rechecks = nullptr;  // MIXED64 FP64 re-decisions
+    tvs::QueueDem *d_qdem = nullptr;           // this context as a one-DEM queue
+    tvs::QueueConfig qcfg{0, 0, 0};            // sweep configuration (autotuned or default)
+    tvs::QueueConfig qcfg_uploaded{0, 0, 0};   // the tiling currently in d_qdem
+    uint32_t q_tiles_per_sector = 0;
+    int32_t *d_deltas = nullptr;
+    float *d_dists = nullptr;
+    // ring output (allocated on first use)
+    uint32_t *d_rings = nullptr;
+    uint4 *d_spill = nullptr;
+    uint32_t *d_counters = nullptr;
+    uint32_t spill_cap = 0;
+    // plain-kernel scratch (allocated on first use)
+    float *d_sf = nullptr, *d_sb = nullptr;
+    // sectors whose shape stage ran since the last tvs_device_finish
+    bool pending[tvs::kSectorSteps] = {};
+    uint64_t device_bytes = 0;  // everything this context allocated on the device
+};
+
+// Helpers capi.cu shares with the other host files of the library.
+void tvs_set_create_error(const std::string &msg);
+namespace tvs_host {
+tvs::ShapeArgs shape_args_of(tvs_context *c, uint32_t first_slot);
+tvs::QueueDem queue_dem_of(const tvs_context *c);
+int header_status_of(tvs_context *c, uint32_t first, uint32_t count);
+}  // namespace tvs_host

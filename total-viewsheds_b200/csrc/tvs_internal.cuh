@@ -102,29 +102,45 @@ struct SweepArgs {
     uint32_t *counters;            // [0] spill count [1] overflow bands [2] max ids
 };
 
-// Persistent sweep over a (sector, tile) work queue (sweep_queue.cu).
-struct QueueArgs {
+// Persistent sweep over a (sector, DEM, tile) work queue (sweep_queue.cu).
+// One DEM of the queue: a context is a batch of one.
+struct QueueDem {
     const float *elev;
     uint32_t width, tvs_width, los;
     uint32_t row_begin, row_end;
     float observer_height;
-    uint32_t first_sector, n_sectors;  // absolute sector slots
     uint32_t step_cap;
-    const ShapeHeader *hdr;            // per-slot arrays (absolute slot index)
+    const ShapeHeader *hdr;            // per sector slot (absolute slot index)
     const float4 *steps;
     const int2 *offs;
     const double4 *dtab;               // FP64 tables {1/d, d/R, d*tan1, 0} (double)
     float *cumulative;
     float *total;                      // nullable
-    double *cumulative64;              // FP64 only
-    uint32_t tiles_x, tiles_y;         // set by the launcher
+    double *cumulative64;              // FP64/MIXED64 only
+    const float *hmax;                 // MIXED64: max |elevation| + |observer height|
+    uint32_t tiles_x, tiles_y;         // set by queue_tile
+    uint32_t tile_base;                // first item of this DEM within a sector
+    uint32_t done_base;                // this DEM's per-tile counters in `done`
+};
+
+struct QueueArgs {
+    const QueueDem *dems;              // device array, tile_base ascending
+    uint32_t n_dems;
+    uint32_t first_sector, n_sectors;  // absolute sector slots
+    uint32_t tiles_per_sector;         // sum of tiles_x * tiles_y
+    uint32_t max_step_cap;
     uint32_t *queue;                   // [1] next work item
     uint32_t *done;                    // [done_cap] sectors completed per tile
-    uint32_t done_cap;
+    uint32_t done_total, done_cap;
     int32_t *error;                    // TVS_ERR_TIMEOUT when a wait gives up
     uint32_t spin_limit;
-    const float *hmax;                 // MIXED64: max |elevation| + |observer height|
     unsigned long long *rechecks;      // MIXED64: FP64 re-decisions (nullable)
+};
+
+// Points of view per thread (columns px 32 apart, rows py 8 apart) and the
+// packed f32x2 arithmetic switch (exact f32 only).
+struct QueueConfig {
+    int px, py, packed;
 };
 
 struct PlainArgs {
@@ -167,8 +183,16 @@ cudaError_t launch_sweep_engine(const SweepArgs &a, int precision, cudaStream_t 
 cudaError_t launch_sweep_const(const SweepArgs &a, int precision, uint32_t n_steps,
                                cudaStream_t s);
 cudaError_t launch_sweep_plain(const PlainArgs &a, cudaStream_t s);
-cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, cudaStream_t s);
+cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, const QueueConfig &c,
+                               cudaStream_t s);
 uint32_t queue_tiles_bound(uint32_t tvs_width, uint32_t rows);
+bool queue_config_valid(const QueueConfig &c);
+QueueConfig default_queue_config();
+// Sets tiles_x/tiles_y/tile_base/done_base of every DEM for the configuration.
+void queue_tile(QueueDem *dems, uint32_t n_dems, const QueueConfig &c, uint32_t *tiles_per_sector,
+                uint32_t *done_total);
+cudaError_t launch_shape_batch(const ShapeArgs *d_args, uint32_t n_dems, uint32_t n_sectors,
+                               cudaStream_t s);
 cudaError_t launch_combine(float *cum, float *total, const float *sf, const float *sb,
                            uint64_t n, cudaStream_t s);
 cudaError_t measure_fp32_issue(double *instructions_per_second);
