@@ -143,7 +143,8 @@ int tvs_set_elevations(tvs_context *ctx, const float *elevations, uint64_t n_ele
 
 /* Axes::compute (axes.rs:103-130) restricted to what the shape needs:
  * sector_ordered[first_rank .. first_rank+count) (ids in sector order) and
- * the f32 sight distances of every point (nullable). */
+ * the f32 sight distances of every point (nullable).  For a rectangular DEM
+ * the order covers the central min(W, H) square the shape is built on. */
 int tvs_axes(tvs_context *ctx, uint32_t angle, uint64_t first_rank, uint64_t count,
              uint32_t *sector_ordered, float *sight_distances);
 

@@ -202,19 +202,56 @@ static int cmp_rank_pos(const void *a, const void *b) {
     return (x > y) - (x < y);
 }
 
+/* The square the band shape is built on: the whole DEM when it is square (the
+ * reference), the central min(W, H) square of a rectangular DEM (the
+ * extension: the reference's construction on the long axis of an elongated
+ * DEM makes strip steps long enough to leave it). */
+static void shape_window(const tvso_geometry *g, uint32_t *side, uint32_t *x0, uint32_t *y0) {
+    uint32_t s = g->width < g->height ? g->width : g->height;
+    *side = s;
+    *x0 = (g->width - s) / 2;
+    *y0 = (g->height - s) / 2;
+}
+
+/* axes.rs:154-176 for one point given by its DEM id. */
+static double projection_of(uint32_t width, uint64_t id, double s, double c) {
+    double y = (double)(-(int64_t)(id / width));
+    double right = y * c;
+    double left = (double)(id % width) * s;
+    return left - right;
+}
+
 /* band_of_sight.rs:61-174 */
 int tvso_compile_band_data(const tvso_geometry *g, float angle, int32_t *deltas,
                            float *dists, uint32_t *n_filled) {
     if (!g || !deltas || !dists) return TVSO_ERR_ARGS;
-    uint64_t n = g->size;
-    float *d32 = malloc(n * sizeof(float));
-    uint32_t *rank = malloc(n * sizeof(uint32_t));
-    uint32_t *sector = malloc(n * sizeof(uint32_t));
+    uint32_t side, x0, y0;
+    shape_window(g, &side, &x0, &y0);
+    const uint64_t n = (uint64_t)side * side;           /* points of the window */
+    const float shifted = angle + SECTOR_SHIFT;         /* axes.rs:95 (f32) */
+    const double ss = sin((double)shifted * RADS_PER_DEG), sc = cos((double)shifted * RADS_PER_DEG);
+    const float sector_angle = shifted + 90.0f;         /* axes.rs:127 */
+    const double ts = sin((double)sector_angle * RADS_PER_DEG);
+    const double tc = cos((double)sector_angle * RADS_PER_DEG);
+    double *d = malloc(n * sizeof(double));
+    uint32_t *ids = malloc(n * sizeof(uint32_t));       /* local index -> DEM id */
+    uint32_t *order = malloc(n * sizeof(uint32_t));
+    uint32_t *rank = malloc(n * sizeof(uint32_t));      /* local index -> sight rank */
+    uint32_t *sector = malloc(n * sizeof(uint32_t));    /* sector rank -> local index */
     rank_pos *window = NULL;
     uint32_t *window_ids = NULL;
     int rc = TVSO_ERR_NOMEM;
-    if (!d32 || !rank || !sector) goto done;
-    rc = axes_compute(g->width, g->height, angle, d32, rank, NULL, sector);
+    if (!d || !ids || !order || !rank || !sector) goto done;
+    /* window points in row-major order (ascending DEM id), as axes.rs:160-172
+     * enumerates a square DEM */
+    for (uint64_t k = 0; k < n; k++)
+        ids[k] = (uint32_t)((uint64_t)(y0 + k / side) * g->width + x0 + k % side);
+    for (uint64_t k = 0; k < n; k++) d[k] = projection_of(g->width, ids[k], ss, sc);
+    rc = tvso_order_by_distance(d, n, order);
+    if (rc) goto done;
+    for (uint64_t r = 0; r < n; r++) rank[order[r]] = (uint32_t)r;
+    for (uint64_t k = 0; k < n; k++) d[k] = projection_of(g->width, ids[k], ts, tc);
+    rc = tvso_order_by_distance(d, n, sector);
     if (rc) goto done;
 
     uint32_t dsize = g->band_deltas_size;
@@ -224,10 +261,10 @@ int tvso_compile_band_data(const tvso_geometry *g, float angle, int32_t *deltas,
     /* :95 (f64 product truncated to usize) */
     uint64_t band_samples =
         (uint64_t)((double)(g->band_size * 2) * DIAGONAL_GREATER_THAN_WIDTH);
-    uint64_t pov_id = n / 2;                              /* :99 */
+    uint64_t pov_local = n / 2;                           /* :99 */
     rc = TVSO_ERR_SHAPE_PANIC;
-    if (band_samples / 2 > pov_id) goto done;             /* :103 usize underflow */
-    uint64_t band_edge = pov_id - band_samples / 2;
+    if (band_samples / 2 > pov_local) goto done;          /* :103 usize underflow */
+    uint64_t band_edge = pov_local - band_samples / 2;
     if (band_edge + band_samples > n) goto done;          /* :113 index */
 
     window = malloc(band_samples * sizeof(rank_pos));
@@ -235,9 +272,9 @@ int tvso_compile_band_data(const tvso_geometry *g, float angle, int32_t *deltas,
     rc = TVSO_ERR_NOMEM;
     if (!window || !window_ids) goto done;
     for (uint64_t i = 0; i < band_samples; i++) {         /* :111-120 */
-        uint32_t dem_id = sector[band_edge + i];
-        window_ids[i] = dem_id;
-        window[i].rank = rank[dem_id];
+        uint32_t local = sector[band_edge + i];
+        window_ids[i] = ids[local];
+        window[i].rank = rank[local];
         window[i].pos = (uint32_t)i;
     }
     /* :135-145 ranks are unique, so any sort gives the same permutation */
@@ -245,7 +282,7 @@ int tvso_compile_band_data(const tvso_geometry *g, float angle, int32_t *deltas,
 
     uint64_t middle = band_samples / 2;                   /* :149 */
     uint64_t end_of_band = (uint64_t)g->band_size * 2;    /* :150 */
-    float pov_distance = d32[pov_id];                     /* :157 */
+    float pov_distance = (float)projection_of(g->width, ids[pov_local], ss, sc);  /* :157 */
     uint32_t filled = 0;
     rc = TVSO_ERR_SHAPE_PANIC;
     for (uint64_t band_id = middle; band_id < end_of_band; band_id++) {
@@ -255,14 +292,14 @@ int tvso_compile_band_data(const tvso_geometry *g, float angle, int32_t *deltas,
         int32_t current = (int32_t)window_ids[window[band_id].pos];
         int32_t next = (int32_t)window_ids[window[band_id + 1].pos];
         deltas[i] = current - next;                       /* :164 */
-        float next_distance = d32[(uint32_t)next];
+        float next_distance = (float)projection_of(g->width, (uint32_t)next, ss, sc);
         dists[i] = fabsf(pov_distance - next_distance);   /* :167-168 */
         filled++;
     }
     if (n_filled) *n_filled = filled;
     rc = TVSO_OK;
 done:
-    free(d32); free(rank); free(sector); free(window); free(window_ids);
+    free(d); free(ids); free(order); free(rank); free(sector); free(window); free(window_ids);
     return rc;
 }
 

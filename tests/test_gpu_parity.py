@@ -256,3 +256,16 @@ def test_shapes_7201(tvs, oracle, angle):
     with tvs.Engine(np.zeros(w * w, np.float32), w, s, los) as eng:
         d1, x1, f1 = eng.band_shape(angle)
     assert f0 == f1 and np.array_equal(d0, d1) and np.array_equal(bits(x0), bits(x1))
+
+
+@pytest.mark.parametrize("w,h,s", [(311, 197, 90.0), (180, 260, 30.0), (640, 301, 30.0)])
+def test_rectangular_shapes_every_sector(tvs, oracle, w, h, s):
+    """Rectangular DEMs build each sector's shape on the central min(W, H) square."""
+    los = int(min(w, h) / 3 * s)
+    g = oracle.geometry(w, s, los, height=h)
+    with tvs.Engine(np.zeros(w * h, np.float32), w, s, los, height=h) as eng:
+        for angle in range(180):
+            d0, x0, f0 = oracle.compile_band_data(g, float(angle))
+            d1, x1, f1 = eng.band_shape(angle)
+            assert f0 == f1 and np.array_equal(d0, d1), angle
+            assert np.array_equal(bits(x0), bits(x1)), angle

@@ -96,3 +96,37 @@ def test_zero_total_bands_is_fine(oracle):
     z = f32(np.arange(81) % 5)
     cum, total, _ = oracle.run(g, z, 1.8, 0, 3)
     assert cum.size == g.computable_points_count
+
+
+@pytest.mark.parametrize("w,h", [(311, 197), (180, 260), (97, 61)])
+def test_rectangular_shapes_stay_on_the_dem(oracle, synth, w, h):
+    """With the line of sight at a third of the shorter side, bands built on the
+    central square never leave a rectangular DEM (every sector runs)."""
+    s = 30.0
+    g = oracle.geometry(w, s, int(min(w, h) / 3 * s), height=h)
+    z = synth.fbm(w, h, 0.8, 3, 0.0, 500.0)
+    cum, _, _ = oracle.run(g, z, 1.65, 0, 180)
+    assert np.isfinite(cum).all() and cum.size == g.tvs_width * g.tvs_height
+
+
+def test_square_window_is_the_whole_dem(oracle):
+    """For a square DEM the window construction is the reference's: rebuild
+    band_of_sight.rs:95-170 from the full sorts of tvso_axes and compare."""
+    g = oracle.geometry(61, 5.0, 100)
+    size = 61 * 61
+    bs = int((2 * g.band_size) * 1.4142135623730951)
+    for angle in (0.0, 37.0, 135.0, 179.0):
+        dist, sight, sector = oracle.axes(61, angle)
+        rank = np.empty(size, np.int64)
+        rank[sight] = np.arange(size)
+        window = sector[size // 2 - bs // 2: size // 2 - bs // 2 + bs]
+        strip = window[np.argsort(rank[window], kind="stable")]
+        m = bs // 2
+        n = 2 * g.band_size - m
+        want_d = np.zeros(g.band_deltas_size, np.int32)
+        want_x = np.zeros(g.band_deltas_size, np.float32)
+        want_d[:n] = strip[m:m + n].astype(np.int64) - strip[m + 1:m + n + 1].astype(np.int64)
+        want_x[:n] = np.abs(dist[size // 2] - dist[strip[m + 1:m + n + 1]])
+        d, x, filled = oracle.compile_band_data(g, angle)
+        assert filled == n
+        assert np.array_equal(d, want_d) and np.array_equal(x.view(np.uint32), want_x.view(np.uint32))

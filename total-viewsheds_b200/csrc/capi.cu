@@ -113,7 +113,9 @@ int derive_geometry(const tvs_params *p, tvs_geometry *g, std::string *msg) {
     const uint64_t bs = (uint64_t)((double)(g->band_size * 2) * kSqrt2);
     g->band_samples = (uint32_t)bs;
     const uint64_t middle = bs / 2, end = 2ull * g->band_size;
-    if (bs / 2 > g->size / 2 || g->size / 2 - bs / 2 + bs > g->size || end >= bs ||
+    // the shape is built on the central min(W, H) square (the whole DEM when square)
+    const uint64_t win = (uint64_t)shorter * shorter;
+    if (bs / 2 > win / 2 || win / 2 - bs / 2 + bs > win || end >= bs ||
         end - middle > g->band_deltas_size) {
         *msg = "line of sight too short for the band-of-sight shape (band_of_sight.rs:103-165 "
                "index out of bounds)";
@@ -145,6 +147,9 @@ tvs::ShapeArgs shape_args(tvs_context *c, uint32_t first_slot) {
     a.width = c->g.width;
     a.height = c->g.height;
     a.size = c->g.size;
+    a.win = std::min(c->g.width, c->g.height);
+    a.x0 = (c->g.width - a.win) / 2;
+    a.y0 = (c->g.height - a.win) / 2;
     a.band_size = c->g.band_size;
     a.band_deltas_size = c->g.band_deltas_size;
     a.band_samples = c->g.band_samples;
@@ -625,7 +630,9 @@ int tvs_set_elevations(tvs_context *ctx, const float *elevations, uint64_t n) {
 int tvs_axes(tvs_context *ctx, uint32_t angle, uint64_t first_rank, uint64_t count,
              uint32_t *sector_ordered, float *sight_distances) {
     if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
-    if (angle >= tvs::kSectorSteps || first_rank + count > ctx->g.size)
+    const uint64_t win = (uint64_t)std::min(ctx->g.width, ctx->g.height) *
+                         std::min(ctx->g.width, ctx->g.height);
+    if (angle >= tvs::kSectorSteps || first_rank + count > win)
         return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "angle or rank range out of bounds");
     TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
     if (sector_ordered && count) {

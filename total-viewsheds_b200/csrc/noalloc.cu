@@ -21,6 +21,7 @@
 // process-wide lock for the whole call and synchronising the stream before it
 // returns.  The first call on a device looks up the array's device address
 // (cudaGetSymbolAddress); make that first call before any stream capture.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -136,6 +137,9 @@ extern "C" int tvs_compute_sector_noalloc(const tvs_params *params, const float 
     a.width = g.width;
     a.height = g.height;
     a.size = g.size;
+    a.win = std::min(g.width, g.height);
+    a.x0 = (g.width - a.win) / 2;
+    a.y0 = (g.height - a.win) / 2;
     a.band_size = g.band_size;
     a.band_deltas_size = bds;
     a.band_samples = g.band_samples;

@@ -41,22 +41,22 @@ __device__ __forceinline__ uint32_t key_at(uint32_t x, double right, double s) {
     return f32_radix_key(projection32(x, right, s));
 }
 
-// Number of x in [0, W) whose key is < K.  Keys are non-decreasing in x when
-// s >= 0 and non-increasing when s < 0.
-__device__ uint32_t row_count_less(uint64_t K, double right, double s, uint32_t W) {
-    uint32_t lo = 0, hi = W;
+// Number of x in [x0, x0 + S) whose key is < K.  Keys are non-decreasing in x
+// when s >= 0 and non-increasing when s < 0.
+__device__ uint32_t row_count_less(uint64_t K, double right, double s, uint32_t x0, uint32_t S) {
+    uint32_t lo = 0, hi = S;
     if (!(s < 0.0)) {
         while (lo < hi) {
             uint32_t mid = (lo + hi) >> 1;
-            if ((uint64_t)key_at(mid, right, s) < K) lo = mid + 1; else hi = mid;
+            if ((uint64_t)key_at(x0 + mid, right, s) < K) lo = mid + 1; else hi = mid;
         }
         return lo;
     }
     while (lo < hi) {
         uint32_t mid = (lo + hi) >> 1;
-        if ((uint64_t)key_at(mid, right, s) < K) hi = mid; else lo = mid + 1;
+        if ((uint64_t)key_at(x0 + mid, right, s) < K) hi = mid; else lo = mid + 1;
     }
-    return W - lo;
+    return S - lo;
 }
 
 template <typename T>
@@ -72,15 +72,15 @@ __device__ T block_sum(T v, T *scratch) {
     return r;
 }
 
-// Sum over all rows of count(key < K) for two thresholds at once.
-__device__ void count_less2(uint64_t K0, uint64_t K1, double c, double s, uint32_t W,
-                            uint32_t H, uint64_t *out0, uint64_t *out1,
+// Sum over the rows of the window of count(key < K), two thresholds at once.
+__device__ void count_less2(uint64_t K0, uint64_t K1, double c, double s, uint32_t x0,
+                            uint32_t y0, uint32_t S, uint64_t *out0, uint64_t *out1,
                             unsigned long long *scratch) {
     unsigned long long a = 0, b = 0;
-    for (uint32_t row = threadIdx.x; row < H; row += blockDim.x) {
-        double right = row_term(row, c);
-        a += row_count_less(K0, right, s, W);
-        b += row_count_less(K1, right, s, W);
+    for (uint32_t r = threadIdx.x; r < S; r += blockDim.x) {
+        double right = row_term(y0 + r, c);
+        a += row_count_less(K0, right, s, x0, S);
+        b += row_count_less(K1, right, s, x0, S);
     }
     *out0 = block_sum(a, scratch);
     *out1 = block_sum(b, scratch + 32);
@@ -150,7 +150,8 @@ __device__ __forceinline__ void shape_sector(const ShapeArgs &a, const uint32_t 
     unsigned long long *win = cand + kCandidateCap;
 
     const SectorTrig tr = a.trig[sector];
-    const uint32_t W = a.width, H = a.height;
+    const uint32_t W = a.width;
+    const uint32_t S = a.win, X0 = a.x0, Y0 = a.y0;
     const uint64_t rank_hi = rank_lo + rank_count - 1;
 
     // 1-2. Keys of ranks rank_lo and rank_hi in the sector order.
@@ -159,24 +160,25 @@ __device__ __forceinline__ void shape_sector(const ShapeArgs &a, const uint32_t 
         uint64_t mid0 = lo0 + ((hi0 - lo0) >> 1);
         uint64_t mid1 = lo1 + ((hi1 - lo1) >> 1);
         uint64_t c0, c1;
-        count_less2(mid0 + 1, mid1 + 1, tr.sector_cos, tr.sector_sin, W, H, &c0, &c1, sm.red);
+        count_less2(mid0 + 1, mid1 + 1, tr.sector_cos, tr.sector_sin, X0, Y0, S, &c0, &c1, sm.red);
         if (lo0 < hi0) { if (c0 > rank_lo) hi0 = mid0; else lo0 = mid0 + 1; }
         if (lo1 < hi1) { if (c1 > rank_hi) hi1 = mid1; else lo1 = mid1 + 1; }
     }
     const uint64_t K_lo = lo0, K_hi = lo1;
     uint64_t less_lo, le_hi;
-    count_less2(K_lo, K_hi + 1, tr.sector_cos, tr.sector_sin, W, H, &less_lo, &le_hi, sm.red);
+    count_less2(K_lo, K_hi + 1, tr.sector_cos, tr.sector_sin, X0, Y0, S, &less_lo, &le_hi, sm.red);
 
     // 3. Gather the candidates (every point with K_lo <= key <= K_hi).
     if (threadIdx.x == 0) { sm.n_cand = 0; sm.status = TVS_OK; }
     __syncthreads();
     const bool inc = !(tr.sector_sin < 0.0);
-    for (uint32_t row = threadIdx.x; row < H; row += blockDim.x) {
+    for (uint32_t r = threadIdx.x; r < S; r += blockDim.x) {
+        const uint32_t row = Y0 + r;
         double right = row_term(row, tr.sector_cos);
-        uint32_t b = row_count_less(K_lo, right, tr.sector_sin, W);
-        uint32_t e = row_count_less(K_hi + 1, right, tr.sector_sin, W);
+        uint32_t b = row_count_less(K_lo, right, tr.sector_sin, X0, S);
+        uint32_t e = row_count_less(K_hi + 1, right, tr.sector_sin, X0, S);
         if (e <= b) continue;
-        uint32_t x0 = inc ? b : W - e;
+        uint32_t x0 = X0 + (inc ? b : S - e);
         uint32_t n = e - b;
         uint32_t at = atomicAdd(&sm.n_cand, n);
         for (uint32_t k = 0; k < n; k++) {
@@ -232,7 +234,9 @@ __device__ __forceinline__ void shape_sector(const ShapeArgs &a, const uint32_t 
     const uint32_t n_steps = n_filled + min(bds - n_filled, 2u);
     long long *soff = reinterpret_cast<long long *>(cand);           // reuse candidates
     float *sdist = reinterpret_cast<float *>(soff + bds + 2);
-    const uint32_t pov_id = (uint32_t)(a.size / 2);
+    // band_of_sight.rs:99: the middle point of the (window's) row-major order
+    const uint64_t pov_local = (uint64_t)S * S / 2;
+    const uint32_t pov_id = (uint32_t)((Y0 + pov_local / S) * (uint64_t)W + X0 + pov_local % S);
     const float pov_distance =
         projection32(pov_id % W, row_term(pov_id / W, tr.sight_cos), tr.sight_sin);
     int32_t *gdel = a.deltas + (uint64_t)sector * bds;
@@ -329,7 +333,8 @@ k_shape(ShapeArgs a, uint64_t rank_lo, uint64_t rank_count, int axes_mode) {
 __global__ void __launch_bounds__(kShapeThreads, 1)
 k_shape_batch(const ShapeArgs *args, uint32_t n_sectors) {
     const ShapeArgs a = args[blockIdx.x / n_sectors];
-    shape_sector(a, blockIdx.x % n_sectors, a.size / 2 - a.band_samples / 2, a.band_samples, 0);
+    const uint64_t m = (uint64_t)a.win * a.win;
+    shape_sector(a, blockIdx.x % n_sectors, m / 2 - a.band_samples / 2, a.band_samples, 0);
 }
 
 // axes.rs:154-189: the f32 sight distance of every point.
@@ -367,7 +372,7 @@ cudaError_t launch_shape(const ShapeArgs &a, uint32_t n_sectors, cudaStream_t s)
         rank_lo = a.dbg_first;
         rank_count = a.dbg_count;
     } else {
-        rank_lo = a.size / 2 - a.band_samples / 2;   // band_of_sight.rs:99-103
+        rank_lo = (uint64_t)a.win * a.win / 2 - a.band_samples / 2;  // band_of_sight.rs:99-103
         rank_count = a.band_samples;
     }
     k_shape<<<n_sectors, kShapeThreads, smem, s>>>(a, rank_lo, rank_count, axes_mode);

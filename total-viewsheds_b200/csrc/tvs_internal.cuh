@@ -61,6 +61,9 @@ constexpr uint32_t kElevationPad = 32 * 8 + 64;
 struct ShapeArgs {
     uint32_t width, height;
     uint64_t size;
+    // The square the shape is built on: the whole DEM when it is square, the
+    // central min(W, H) square otherwise (columns [x0, x0+win), rows [y0, y0+win)).
+    uint32_t win, x0, y0;
     uint32_t band_size, band_deltas_size, band_samples;
     uint32_t first_angle;      // sector of blockIdx.x == 0
     uint32_t step_cap;         // per-sector stride of the step tables
