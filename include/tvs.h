@@ -155,7 +155,9 @@ int tvs_band_shape(tvs_context *ctx, uint32_t angle, int32_t *band_deltas,
 
 /* Compute::compute_sector (compute.rs:181-203) for ComputeType::Cuda:
  * cumulative_surfaces [computable_points_count] is read, advanced by this
- * sector and written back (kernel.rs:254).  rings (nullable) receives the
+ * sector and written back (kernel.rs:254).  FP64 and MIXED64 contexts widen
+ * the f32 input and accumulate the sector in double (tvs_run keeps double
+ * across sectors).  rings (nullable) receives the
  * sector's ring records in the reference layout; rings_len must be at least
  * ring_slots_per_sector.  stats is nullable. */
 int tvs_compute_sector(tvs_context *ctx, uint32_t angle, float *cumulative_surfaces,

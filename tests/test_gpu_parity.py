@@ -269,3 +269,21 @@ def test_rectangular_shapes_every_sector(tvs, oracle, w, h, s):
             d1, x1, f1 = eng.band_shape(angle)
             assert f0 == f1 and np.array_equal(d0, d1), angle
             assert np.array_equal(bits(x0), bits(x1)), angle
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed64"])
+def test_fp64_compute_sector_matches_oracle(tvs, oracle, dem1201, precision):
+    """One sector in double from the caller's f32 surfaces, with ring records."""
+    w, s, los = PLAIN_GPU
+    angle = 45
+    g = oracle.geometry(w, s, los)
+    deltas, dists, _ = oracle.compile_band_data(g, float(angle))
+    c0 = np.zeros(g.computable_points_count, np.float64)
+    r0 = np.zeros(oracle.ring_len(g), np.uint32)
+    oracle.compute_sector(g, dem1201, 1.65, deltas, dists, c0, r0, f64=True)
+    with tvs.Engine(dem1201, w, s, los, observer_height=1.65, precision=precision) as eng:
+        c1 = np.zeros(eng.count, np.float32)
+        r1 = np.zeros(eng.geometry.ring_slots_per_sector, np.uint32)
+        eng.compute_sector(angle, c1, r1)
+    assert np.array_equal(bits(c0.astype(np.float32)), bits(c1))
+    assert np.array_equal(r0, r1)

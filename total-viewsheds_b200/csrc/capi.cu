@@ -710,12 +710,12 @@ int tvs_compute_sector(tvs_context *ctx, uint32_t angle, float *cumulative_surfa
         return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "rings_len is smaller than one sector's slots");
     TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
     const uint64_t count = ctx->g.computable_points_count;
-    if (ctx->p.precision != TVS_PRECISION_EXACT32)
-        return fail(ctx, TVS_ERR_INVALID_ARGUMENT,
-                    "tvs_compute_sector keeps f32 cumulative surfaces; use tvs_run for FP64/MIXED64");
     if (count)
         TVS_CUDA(ctx, cudaMemcpyAsync(ctx->d_cum, cumulative_surfaces, count * sizeof(float),
                                       cudaMemcpyHostToDevice, ctx->stream));
+    // FP64/MIXED64 accumulate in double within the sector, from the caller's f32
+    if (ctx->d_cum64 && count)
+        TVS_CUDA(ctx, tvs::launch_widen(ctx->d_cum, ctx->d_cum64, count, ctx->stream));
     if (rings) {
         int rc = ensure_rings(ctx);
         if (rc) return rc;

@@ -471,7 +471,18 @@ __global__ void k_max_abs(const float *x, uint64_t n, float add, unsigned int *o
     if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(__fadd_ru(m, fabsf(add))));
 }
 
+__global__ void k_widen(const float *x, double *y, uint64_t n) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = (double)x[i];
+}
+
 }  // namespace
+
+cudaError_t launch_widen(const float *x, double *y, uint64_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    k_widen<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(x, y, n);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_max_abs(const float *x, uint64_t n, float add, float *out, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(out, 0, sizeof(float), s);

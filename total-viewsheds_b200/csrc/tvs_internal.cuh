@@ -199,6 +199,8 @@ cudaError_t launch_shape_batch(const ShapeArgs *d_args, uint32_t n_dems, uint32_
 cudaError_t launch_combine(float *cum, float *total, const float *sf, const float *sb,
                            uint64_t n, cudaStream_t s);
 cudaError_t measure_fp32_issue(double *instructions_per_second);
+// y[i] = (double)x[i]
+cudaError_t launch_widen(const float *x, double *y, uint64_t n, cudaStream_t s);
 // out[0] = max |x[i]| + |add| over n floats (out must hold 1 float).
 cudaError_t launch_max_abs(const float *x, uint64_t n, float add, float *out, cudaStream_t s);
 cudaError_t launch_selftest_division(uint64_t n, uint64_t seed, unsigned long long *mismatches,
