@@ -276,7 +276,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--config", default="precision")
-    ap.add_argument("--precision", default="exact32")
+    ap.add_argument("--precision", default="mixed64",
+                    help="mixed64 (headline), exact32 (the reference's f32 arithmetic) or fp64")
     ap.add_argument("--kernel", default="engine")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -400,33 +401,49 @@ def main():
                "d2h_bytes_per_step": int(2 * g.computable_points_count * 4),
                "ms_per_step": e2e_ms / args.steps}
 
-    # the plain one-thread-per-band port of the reference shader, same GPU
-    plain = None
-    if not args.no_plain and args.kernel == "engine" and args.precision == "exact32":
+    def time_one_tvs(engine):
+        """Device time of one full TVS on `engine` (after one untimed TVS)."""
+        engine.device_reset()
+        engine.device_run_sectors(0, SECTORS)
+        engine.device_finish()
+        es = torch.cuda.ExternalStream(engine.stream(), device=dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(es):
+            flush.fill_(1)
+            e0.record(es)
+            engine.device_reset()
+            engine.device_run_sectors(0, SECTORS)
+            e1.record(es)
+        e1.synchronize()
+        engine.device_finish()
+        return e0.elapsed_time(e1) * 1e-3
+
+    # the FP32 legs of "mixed vs FP32" on the same GPU: the exact-f32 engine
+    # (the reference's arithmetic, bit for bit) and the plain one-thread-per-
+    # band port of the reference shader
+    fp32_engine = plain = None
+    if not args.no_plain and args.kernel == "engine":
+        kw = dict(observer_height=cfg["observer_height"], rings_per_km=cfg["rings_per_km"],
+                  device=local)
         with tvs.Engine(z, cfg["width"], cfg["scale"], cfg["max_line_of_sight"],
-                        observer_height=cfg["observer_height"], rings_per_km=cfg["rings_per_km"],
-                        sweep_kernel="plain", device=local) as pe:
-            pe.device_reset()
-            pe.device_run_sectors(0, SECTORS)
-            pe.device_finish()
-            ps = torch.cuda.ExternalStream(pe.stream(), device=dev)
-            p0 = torch.cuda.Event(enable_timing=True)
-            p1 = torch.cuda.Event(enable_timing=True)
-            with torch.cuda.stream(ps):
-                flush.fill_(1)
-                p0.record(ps)
-                pe.device_reset()
-                pe.device_run_sectors(0, SECTORS)
-                p1.record(ps)
-            p1.synchronize()
-            pe.device_finish()
-            pms = p0.elapsed_time(p1)
+                        precision="exact32", **kw) as e32:
+            t32 = time_one_tvs(e32)
+            c32, _ = e32.read_surfaces()
+        with tvs.Engine(z, cfg["width"], cfg["scale"], cfg["max_line_of_sight"],
+                        sweep_kernel="plain", **kw) as pe:
+            tpl = time_one_tvs(pe)
             c_plain, _ = pe.read_surfaces()
-        c_eng, _ = eng.read_surfaces()
-        plain = {"value": ref_samples / (pms * 1e-3), "s_per_tvs": pms * 1e-3,
-                 "kernel": "one thread per band, IEEE divisions, every delta-table step",
-                 "identical_surfaces": bool(np.array_equal(c_plain.view(np.uint32),
-                                                           c_eng.view(np.uint32)))}
+        c_head, _ = eng.read_surfaces()
+        fp32_engine = {"value": ref_samples / t32, "s_per_tvs": t32,
+                       "kernel": "k_sweep_queue<exact32>: the reference's f32 arithmetic",
+                       "identical_to_plain_port": bool(np.array_equal(c32.view(np.uint32),
+                                                                      c_plain.view(np.uint32)))}
+        plain = {"value": ref_samples / tpl, "s_per_tvs": tpl,
+                 "kernel": "one thread per band, IEEE divisions, every delta-table step"}
+        if args.precision == "exact32":
+            fp32_engine["identical_to_headline"] = bool(np.array_equal(c32.view(np.uint32),
+                                                                       c_head.view(np.uint32)))
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -476,7 +493,7 @@ def main():
                                "(tvs_measure_fp32_issue), run before the timed region",
             },
             "cpu_baseline": base, "e2e": e2e, "gpu_launches": gpu_launches,
-            "plain_fp32_sweep": plain,
+            "fp32_exact_engine": fp32_engine, "plain_fp32_sweep": plain,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

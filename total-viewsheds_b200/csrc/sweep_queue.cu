@@ -153,7 +153,7 @@ __device__ __forceinline__ void step_f64(Chain<kPrec> &c, float h, double hp, fl
 // view per thread it is held to 64 registers (4 CTAs per SM).
 template <int kPrec, int kPx, int kPy>
 constexpr int queue_min_blocks() {
-    return (kPrec == TVS_PRECISION_MIXED64 && kPx * kPy <= 2) ? 4 : 1;
+    return (kPrec == TVS_PRECISION_MIXED64 && kPx * kPy <= 2) ? (kPx * kPy == 1 ? 4 : 3) : 1;
 }
 
 template <int kPrec, int kPx, int kPy, bool kPacked>
@@ -298,7 +298,7 @@ k_sweep_queue(QueueArgs a) {
                     const float4 t = s_steps[i];
                     const long long bo = s_boff[i];
                     const double w64 = s_dtab[i].z;
-                    uint32_t amb = 0;  // one bit per chain
+                    bool any_amb = false;
 #pragma unroll
                     for (int py = 0; py < kPy; py++) {
                         const float *pf = (const float *)((const char *)ep[py] + bo);
@@ -318,20 +318,29 @@ k_sweep_queue(QueueArgs a) {
                                     c.j = (int32_t)i;
                                     c.s = __dadd_rn(c.s, w64);
                                 }
-                                amb |= (uint32_t)am << ((py * kPx + px) * 2 + dir);
+                                any_amb |= am;
                             }
                         }
                     }
-                    if (__any_sync(0xffffffffu, amb != 0)) {
-                        if (amb && a.rechecks) atomicAdd(a.rechecks, (unsigned long long)__popc(amb));
+                    if (__any_sync(0xffffffffu, any_amb)) {
+                        // Re-derive which chains were ambiguous: a chain that was
+                        // surely visible at this step has j == i and is skipped;
+                        // every other chain still has the state it was tested with.
 #pragma unroll
                         for (int py = 0; py < kPy; py++)
 #pragma unroll
                             for (int px = 0; px < kPx; px++)
 #pragma unroll
                                 for (int dir = 0; dir < 2; dir++) {
-                                    if (!((amb >> ((py * kPx + px) * 2 + dir)) & 1u)) continue;
                                     auto &c = dir ? cb[py][px] : cf[py][px];
+                                    if (c.j == (int32_t)i) continue;
+                                    const long long bi = dir ? -bo : bo;
+                                    const float h = __ldg((const float *)((const char *)ep[py] + bi) +
+                                                          kTileX * px);
+                                    const float ah = __fmaf_rn(__fsub_rn(h, hp32[py][px]), t.x, t.z);
+                                    const float dd = __fsub_rn(ah, c.m32);
+                                    if (!(fabsf(dd) <= __fadd_rn(t.w, c.gm))) continue;
+                                    if (a.rechecks) atomicAdd(a.rechecks, 1ull);
                                     if (c.j >= 0) {  // the exact FP64 angle at the maximum
                                         c.m = exact_angle(py, px, dir, (uint32_t)c.j);
                                         c.j = -1;
@@ -339,11 +348,8 @@ k_sweep_queue(QueueArgs a) {
                                     const double a64 = exact_angle(py, px, dir, i);
                                     if (a64 > c.m) {
                                         c.m = a64;
-                                        const long long bi = dir ? -bo : bo;
-                                        const float h = __ldg((const float *)((const char *)ep[py] + bi) +
-                                                              kTileX * px);
-                                        c.m32 = __fmaf_rn(__fsub_rn(h, hp32[py][px]), t.x, t.z);
-                                        c.gm = __fmaf_rn(fabsf(c.m32), 0x1p-19f, t.w);
+                                        c.m32 = ah;
+                                        c.gm = __fmaf_rn(fabsf(ah), 0x1p-19f, t.w);
                                         c.s = __dadd_rn(c.s, w64);
                                     }
                                 }
