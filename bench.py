@@ -453,7 +453,8 @@ def main():
         clk = clocks.summary()
         sweep_avg_s = statistics.mean(sweep_ms) * 1e-3
         achieved = eval_samples * 5 / sweep_avg_s           # FP32 lane-instructions / s
-        traffic = traffic_from_profiles("k_sweep_queue") if args.kernel == "engine" else None
+        traffic = (traffic_from_profiles(f"k_sweep_queue<{args.precision}>")
+                   if args.kernel == "engine" else None)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,

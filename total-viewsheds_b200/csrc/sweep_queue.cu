@@ -153,7 +153,7 @@ __device__ __forceinline__ void step_f64(Chain<kPrec> &c, float h, double hp, fl
 // view per thread it is held to 64 registers (4 CTAs per SM).
 template <int kPrec, int kPx, int kPy>
 constexpr int queue_min_blocks() {
-    return (kPrec == TVS_PRECISION_MIXED64 && kPx * kPy <= 2) ? (kPx * kPy == 1 ? 4 : 3) : 1;
+    return (kPrec == TVS_PRECISION_MIXED64 && kPx * kPy <= 2) ? 4 : 1;
 }
 
 template <int kPrec, int kPx, int kPy, bool kPacked>
