@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define TVS_ABI_VERSION 1
+#define TVS_ABI_VERSION 2
 
 /* Status codes.  Negative values are errors; tvs_last_error() has the text. */
 enum tvs_status {
@@ -204,11 +204,14 @@ uint64_t tvs_device_bytes(const tvs_context *ctx);
 /* Points of view per thread of the persistent sweep: points_x columns 32
  * apart times points_y rows 8 apart (1x1, 2x1, 4x1, 2x2, 8x1), i.e. a CTA tile
  * of 32*points_x x 8*points_y points; packed != 0 selects the packed f32x2
- * arithmetic (exact f32 only).  Results do not depend on it. */
+ * arithmetic (exact f32 only); prefetch != 0 issues the next step's elevation
+ * loads before the current step's arithmetic (not with packed).  Results do
+ * not depend on any of them. */
 typedef struct tvs_sweep_config {
     int32_t points_x;
     int32_t points_y;
     int32_t packed;
+    int32_t prefetch;
 } tvs_sweep_config;
 
 int tvs_set_sweep_config(tvs_context *ctx, const tvs_sweep_config *cfg);

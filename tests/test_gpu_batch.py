@@ -67,12 +67,28 @@ def test_batch_autotune_keeps_results(tvs, tiles):
             assert np.array_equal(bits(bc), bits(c)) and np.array_equal(bits(bt), bits(t))
 
 
-@pytest.mark.parametrize("shape", [(1, 1, 0), (4, 1, 0), (2, 2, 0), (8, 1, 0), (2, 1, 1), (4, 1, 1)])
+@pytest.mark.parametrize("shape", [(1, 1, 0), (4, 1, 0), (2, 2, 0), (8, 1, 0), (2, 1, 1), (4, 1, 1),
+                                   (1, 1, 0, 1), (2, 1, 0, 1), (4, 1, 0, 1), (2, 2, 0, 1),
+                                   (8, 1, 0, 1)])
 def test_sweep_configurations_agree(tvs, synth, shape):
     z = synth.config_dem("plain_cpu")
     with tvs.Engine(z, 301, 30.0, 3000, observer_height=1.65) as eng:
         want, wt, _ = eng.run()
         eng.set_sweep_config(*shape)
+        got, gt, _ = eng.run()
+    assert np.array_equal(bits(want), bits(got)) and np.array_equal(bits(wt), bits(gt))
+
+
+@pytest.mark.parametrize("precision", ["mixed64", "fp64"])
+@pytest.mark.parametrize("shape", [(1, 1), (2, 1), (4, 1), (2, 2)])
+def test_prefetch_configurations_agree_wide(tvs, synth, precision, shape):
+    """The prefetching sweep gives the default sweep's FP64 and MIXED64
+    results bit for bit."""
+    z = synth.config_dem("plain_cpu")
+    with tvs.Engine(z, 301, 30.0, 3000, observer_height=1.65, precision=precision) as eng:
+        want, wt, _ = eng.run()
+        eng.set_sweep_config(*shape, prefetch=True)
+        assert eng.sweep_config().prefetch == 1
         got, gt, _ = eng.run()
     assert np.array_equal(bits(want), bits(got)) and np.array_equal(bits(wt), bits(gt))
 

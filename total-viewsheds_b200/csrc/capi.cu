@@ -828,7 +828,7 @@ const float *tvs_device_cumulative(const tvs_context *ctx) { return ctx ? ctx->d
 
 int tvs_set_sweep_config(tvs_context *ctx, const tvs_sweep_config *cfg) {
     if (!ctx || !cfg) return TVS_ERR_INVALID_ARGUMENT;
-    tvs::QueueConfig c{cfg->points_x, cfg->points_y, cfg->packed != 0};
+    tvs::QueueConfig c{cfg->points_x, cfg->points_y, cfg->packed != 0, cfg->prefetch != 0};
     if (!tvs::queue_config_valid(c))
         return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "unsupported points-per-thread shape");
     ctx->qcfg = c;
@@ -840,6 +840,7 @@ int tvs_get_sweep_config(const tvs_context *ctx, tvs_sweep_config *cfg) {
     cfg->points_x = ctx->qcfg.px;
     cfg->points_y = ctx->qcfg.py;
     cfg->packed = ctx->qcfg.packed;
+    cfg->prefetch = ctx->qcfg.prefetch;
     return TVS_OK;
 }
 
@@ -849,8 +850,9 @@ int tvs_autotune(tvs_context *ctx, uint32_t sample_sectors, tvs_sweep_config *ch
         return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "sample_sectors must be in [1, 180]");
     TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
     const bool exact = ctx->p.precision == TVS_PRECISION_EXACT32;
-    const tvs::QueueConfig cands[] = {{1, 1, 0}, {2, 1, 0}, {4, 1, 0}, {2, 2, 0},
-                                      {2, 1, 1}, {4, 1, 1}};
+    const tvs::QueueConfig cands[] = {{1, 1, 0, 0}, {2, 1, 0, 0}, {4, 1, 0, 0}, {2, 2, 0, 0},
+                                      {2, 1, 1, 0}, {4, 1, 1, 0}, {1, 1, 0, 1}, {2, 1, 0, 1},
+                                      {4, 1, 0, 1}, {2, 2, 0, 1}};
     cudaEvent_t t0, t1;
     TVS_CUDA(ctx, cudaEventCreate(&t0));
     TVS_CUDA(ctx, cudaEventCreate(&t1));

@@ -114,15 +114,21 @@ template <> struct Chain<TVS_PRECISION_FP64> {
     double m, s;
     __device__ void init() { m = -2000.0; s = 0.0; }
 };
-// MIXED64: m is the FP64 running maximum, s the FP64 surface; m32 is the FP32
-// estimate of the angle at the maximum and gm the part of the decision window
-// that belongs to it.  j >= 0: m is stale and is recomputed from step j when a
-// comparison needs it; j < 0: m is exact.
+// MIXED64: s is the FP64 surface; m32 is the FP32 estimate of the angle at the
+// running maximum, gm the part of the decision window that belongs to it and
+// lo = m32 - gm the filter threshold.  The FP64 maximum is the exact angle at
+// step j (the last step that raised it; -2000 while j < 0): it is recomputed
+// when a comparison needs it and held in m only for the tail steps.
 template <> struct Chain<TVS_PRECISION_MIXED64> {
     double m, s;
-    float m32, gm;
+    float m32, gm, lo;
     int32_t j;
-    __device__ void init() { m = -2000.0; s = 0.0; m32 = -2000.0f; gm = 0.0f; j = -1; }
+    __device__ void init() { m = -2000.0; s = 0.0; m32 = -2000.0f; gm = 0.0f; lo = -2000.0f; j = -1; }
+    __device__ void set_max32(float ah, float g) {
+        m32 = ah;
+        gm = __fmaf_rn(fabsf(ah), 0x1p-19f, g);
+        lo = __fsub_rn(m32, gm);
+    }
 };
 
 template <int kPrec, bool kFast>
@@ -149,16 +155,27 @@ __device__ __forceinline__ void step_f64(Chain<kPrec> &c, float h, double hp, fl
     c.m = fmax(a, c.m);
 }
 
-// MIXED64 carries 7 registers of state per chain; with one or two points of
-// view per thread it is held to 64 registers (4 CTAs per SM).
+// MIXED64 carries 6 registers of state per chain; with one or two points of
+// view per thread it is held to 64 registers (4 CTAs per SM), with four to 128
+// (2 CTAs per SM).
+#ifndef TVS_MIX_MIN_BLOCKS
+#define TVS_MIX_MIN_BLOCKS 4
+#endif
 template <int kPrec, int kPx, int kPy>
 constexpr int queue_min_blocks() {
-    return (kPrec == TVS_PRECISION_MIXED64 && kPx * kPy <= 2) ? 4 : 1;
+    return kPrec != TVS_PRECISION_MIXED64 ? 1
+           : kPx * kPy <= 2               ? TVS_MIX_MIN_BLOCKS
+           : kPx * kPy == 4               ? 2
+                                          : 1;
 }
 
-template <int kPrec, int kPx, int kPy, bool kPacked>
+// kVar: 0 scalar, 1 packed f32x2 (exact f32 only), 2 scalar with the next
+// step's elevations loaded while the current step computes.
+template <int kPrec, int kPx, int kPy, int kVar>
 __global__ void __launch_bounds__(kThreads, (queue_min_blocks<kPrec, kPx, kPy>()))
 k_sweep_queue(QueueArgs a) {
+    constexpr bool kPacked = kVar == 1;
+    constexpr bool kPipe = kVar == 2;
     constexpr bool kMix = kPrec == TVS_PRECISION_MIXED64;
     constexpr bool kF64 = kPrec == TVS_PRECISION_FP64 || kMix;  // FP64 tables and surfaces
     extern __shared__ __align__(16) unsigned char smem[];
@@ -212,14 +229,18 @@ k_sweep_queue(QueueArgs a) {
                 if (kMix) {
                     // decision window of the FP32 estimate at this step: at least 4x
                     // the bound 2^-22 (|a| + d/R + hmax/d) on |estimate - FP64 angle|
-                    // (the |a| part is carried with the running maximum)
+                    // (the |a| part is carried with the running maximum).  The
+                    // filter's offset -d/R + g takes the place of d, which moves
+                    // to the FP64 table.
                     const float g = __fadd_rn(__fmul_rn(0x1p-20f, __fadd_rn(t.z, __fmul_rn(hmax, t.x))),
                                               0x1p-90f);
-                    s_steps[i] = make_float4(t.x, t.y, -t.z, g);
+                    s_steps[i] = make_float4(t.x, __fadd_rn(-t.z, g), -t.z, g);
                 }
                 s_boff[i] = (long long)go[i].x * (long long)sizeof(float);
                 if (kF64) {
-                    s_dtab[i] = D.dtab[(uint64_t)slot * D.step_cap + i];
+                    double4 dv = D.dtab[(uint64_t)slot * D.step_cap + i];
+                    if (kMix) dv.w = (double)t.y;
+                    s_dtab[i] = dv;
                 } else if (kPacked) {  // only the packed loop reserves these 32 B per step
                     PackedStep p;
                     p.y = pk(t.x, t.x);
@@ -282,6 +303,14 @@ k_sweep_queue(QueueArgs a) {
                     cb[py][px].init();
                 }
             }
+            // MIXED64 reloads the FP64 observer elevation where it needs it (the
+            // rare re-decisions and the tail) instead of holding it
+            auto hp_of = [&](int py, int px) -> HP {
+                if constexpr (kMix)
+                    return (HP)__dadd_rn((double)__ldg(ep[py] + kTileX * px), (double)D.observer_height);
+                else
+                    return hp[py][px];
+            };
             uint32_t i = 0;
             if constexpr (kMix) {
                 // FP32 estimate per sample; FP64 only for comparisons inside the
@@ -290,38 +319,86 @@ k_sweep_queue(QueueArgs a) {
                 auto exact_angle = [&](int py, int px, int dir, uint32_t k) -> double {
                     const long long bk = s_boff[k];
                     const float *pk_ = (const float *)((const char *)ep[py] + (dir ? -bk : bk));
-                    const double ek = __dsub_rn((double)__ldg(pk_ + kTileX * px), hp[py][px]);
+                    const double ek = __dsub_rn((double)__ldg(pk_ + kTileX * px), hp_of(py, px));
                     const double4 dk = s_dtab[k];
-                    return __dsub_rn(div_table64(ek, dk.x, (double)s_steps[k].y), dk.y);
+                    return __dsub_rn(div_table64(ek, dk.x, dk.w), dk.y);
                 };
+                auto max64 = [&](int py, int px, int dir, int32_t j) -> double {
+                    return j < 0 ? -2000.0 : exact_angle(py, px, dir, (uint32_t)j);
+                };
+                // elevations of this step (and, pipelined, of the next one)
+                float hc[2][kPy][kPx], hn[2][kPy][kPx];
+                auto load_step = [&](float (&h)[2][kPy][kPx], long long b) {
+#pragma unroll
+                    for (int py = 0; py < kPy; py++)
+#pragma unroll
+                        for (int px = 0; px < kPx; px++) {
+                            h[0][py][px] = __ldg((const float *)((const char *)ep[py] + b) + kTileX * px);
+                            h[1][py][px] = __ldg((const float *)((const char *)ep[py] - b) + kTileX * px);
+                        }
+                };
+                if (kPipe && n_fast > 0) load_step(hn, s_boff[0]);
                 for (; i < n_fast; i++) {
                     const float4 t = s_steps[i];
-                    const long long bo = s_boff[i];
+                    if constexpr (kPipe) {
+#pragma unroll
+                        for (int dir = 0; dir < 2; dir++)
+#pragma unroll
+                            for (int py = 0; py < kPy; py++)
+#pragma unroll
+                                for (int px = 0; px < kPx; px++) hc[dir][py][px] = hn[dir][py][px];
+                        load_step(hn, s_boff[min(i + 1, n_fast - 1)]);
+                    } else {
+                        load_step(hc, s_boff[i]);
+                    }
+                    // Filter: a chain can change state at this step only if
+                    // estimate + g >= m32 - gm, a superset of the surely-visible
+                    // (dd > g) and ambiguous (|dd| <= g) cases below; the window's
+                    // slack covers the two extra roundings.  Most steps of most
+                    // warps stop here.
+                    float es[2][kPy][kPx];
+                    bool hit = false;
+#pragma unroll
+                    for (int py = 0; py < kPy; py++)
+#pragma unroll
+                        for (int px = 0; px < kPx; px++)
+#pragma unroll
+                            for (int dir = 0; dir < 2; dir++) {
+                                const auto &c = dir ? cb[py][px] : cf[py][px];
+                                const float e = __fsub_rn(hc[dir][py][px], hp32[py][px]);
+                                es[dir][py][px] = e;
+                                hit |= __fmaf_rn(e, t.x, t.y) >= c.lo;
+                            }
+                    if (!__any_sync(0xffffffffu, hit)) continue;
+                    float ahs[2][kPy][kPx], dds[2][kPy][kPx];
+#pragma unroll
+                    for (int py = 0; py < kPy; py++)
+#pragma unroll
+                        for (int px = 0; px < kPx; px++)
+#pragma unroll
+                            for (int dir = 0; dir < 2; dir++) {
+                                const auto &c = dir ? cb[py][px] : cf[py][px];
+                                ahs[dir][py][px] = __fmaf_rn(es[dir][py][px], t.x, t.z);
+                                dds[dir][py][px] = __fsub_rn(ahs[dir][py][px], c.m32);
+                            }
                     const double w64 = s_dtab[i].z;
                     bool any_amb = false;
 #pragma unroll
-                    for (int py = 0; py < kPy; py++) {
-                        const float *pf = (const float *)((const char *)ep[py] + bo);
-                        const float *pb = (const float *)((const char *)ep[py] - bo);
+                    for (int py = 0; py < kPy; py++)
 #pragma unroll
-                        for (int px = 0; px < kPx; px++) {
+                        for (int px = 0; px < kPx; px++)
 #pragma unroll
                             for (int dir = 0; dir < 2; dir++) {
                                 auto &c = dir ? cb[py][px] : cf[py][px];
-                                const float h = __ldg((dir ? pb : pf) + kTileX * px);
-                                const float ah = __fmaf_rn(__fsub_rn(h, hp32[py][px]), t.x, t.z);
-                                const float dd = __fsub_rn(ah, c.m32);
+                                const float ah = ahs[dir][py][px], dd = dds[dir][py][px];
                                 const bool am = fabsf(dd) <= __fadd_rn(t.w, c.gm);
                                 if (!am && dd > 0.0f) {  // surely visible
-                                    c.m32 = ah;
-                                    c.gm = __fmaf_rn(fabsf(ah), 0x1p-19f, t.w);
+                                    c.set_max32(ah, t.w);
                                     c.j = (int32_t)i;
                                     c.s = __dadd_rn(c.s, w64);
                                 }
                                 any_amb |= am;
                             }
-                        }
-                    }
                     if (__any_sync(0xffffffffu, any_amb)) {
                         // Re-derive which chains were ambiguous: a chain that was
                         // surely visible at this step has j == i and is skipped;
@@ -334,22 +411,13 @@ k_sweep_queue(QueueArgs a) {
                                 for (int dir = 0; dir < 2; dir++) {
                                     auto &c = dir ? cb[py][px] : cf[py][px];
                                     if (c.j == (int32_t)i) continue;
-                                    const long long bi = dir ? -bo : bo;
-                                    const float h = __ldg((const float *)((const char *)ep[py] + bi) +
-                                                          kTileX * px);
-                                    const float ah = __fmaf_rn(__fsub_rn(h, hp32[py][px]), t.x, t.z);
-                                    const float dd = __fsub_rn(ah, c.m32);
+                                    const float ah = ahs[dir][py][px], dd = dds[dir][py][px];
                                     if (!(fabsf(dd) <= __fadd_rn(t.w, c.gm))) continue;
                                     if (a.rechecks) atomicAdd(a.rechecks, 1ull);
-                                    if (c.j >= 0) {  // the exact FP64 angle at the maximum
-                                        c.m = exact_angle(py, px, dir, (uint32_t)c.j);
-                                        c.j = -1;
-                                    }
                                     const double a64 = exact_angle(py, px, dir, i);
-                                    if (a64 > c.m) {
-                                        c.m = a64;
-                                        c.m32 = ah;
-                                        c.gm = __fmaf_rn(fabsf(ah), 0x1p-19f, t.w);
+                                    if (a64 > max64(py, px, dir, c.j)) {
+                                        c.j = (int32_t)i;
+                                        c.set_max32(ah, t.w);
                                         c.s = __dadd_rn(c.s, w64);
                                     }
                                 }
@@ -363,10 +431,52 @@ k_sweep_queue(QueueArgs a) {
 #pragma unroll
                         for (int dir = 0; dir < 2; dir++) {
                             auto &c = dir ? cb[py][px] : cf[py][px];
-                            if (c.j < 0) continue;
-                            c.m = exact_angle(py, px, dir, (uint32_t)c.j);
-                            c.j = -1;
+                            c.m = max64(py, px, dir, c.j);
                         }
+            } else if constexpr (kPipe) {
+                float nf[kPy][kPx], nb[kPy][kPx];  // the next step's elevations
+                if (n_fast > 0) {
+                    const long long b0 = s_boff[0];
+#pragma unroll
+                    for (int py = 0; py < kPy; py++)
+#pragma unroll
+                        for (int px = 0; px < kPx; px++) {
+                            nf[py][px] = __ldg((const float *)((const char *)ep[py] + b0) + kTileX * px);
+                            nb[py][px] = __ldg((const float *)((const char *)ep[py] - b0) + kTileX * px);
+                        }
+                }
+#pragma unroll 2
+                for (; i < n_fast; i++) {
+                    const float4 t = s_steps[i];
+                    double4 dt;
+                    if (kF64) dt = s_dtab[i];
+                    float hf[kPy][kPx], hb[kPy][kPx];
+                    const long long bn = s_boff[min(i + 1, n_fast - 1)];
+#pragma unroll
+                    for (int py = 0; py < kPy; py++) {
+                        const float *pf = (const float *)((const char *)ep[py] + bn);
+                        const float *pb = (const float *)((const char *)ep[py] - bn);
+#pragma unroll
+                        for (int px = 0; px < kPx; px++) {
+                            hf[py][px] = nf[py][px];
+                            hb[py][px] = nb[py][px];
+                            nf[py][px] = __ldg(pf + kTileX * px);
+                            nb[py][px] = __ldg(pb + kTileX * px);
+                        }
+                    }
+#pragma unroll
+                    for (int py = 0; py < kPy; py++)
+#pragma unroll
+                        for (int px = 0; px < kPx; px++) {
+                            if constexpr (kF64) {
+                                step_f64<kPrec, true>(cf[py][px], hf[py][px], hp[py][px], t.y, dt, 0);
+                                step_f64<kPrec, true>(cb[py][px], hb[py][px], hp[py][px], t.y, dt, 0);
+                            } else {
+                                step_f32<kPrec, true>(cf[py][px], hf[py][px], hp[py][px], t, 0);
+                                step_f32<kPrec, true>(cb[py][px], hb[py][px], hp[py][px], t, 0);
+                            }
+                        }
+                }
             } else if constexpr (kF64 || !kPacked) {
 #pragma unroll 2
                 for (; i < n_fast; i++) {
@@ -441,10 +551,11 @@ k_sweep_queue(QueueArgs a) {
             for (; i < n; i++) {
                 const float4 t = s_steps[i];
                 const long long bo = s_boff[i];
-                // outside the table-division domain (the zero distances)
-                const int slow = !(t.y >= 0x1p-20f && t.y <= 0x1p20f);
                 double4 dt;
                 if (kF64) dt = s_dtab[i];
+                const float dist = kMix ? (float)dt.w : t.y;  // MIXED64 keeps d in the FP64 table
+                // outside the table-division domain (the zero distances)
+                const int slow = !(dist >= 0x1p-20f && dist <= 0x1p20f);
 #pragma unroll
                 for (int py = 0; py < kPy; py++) {
                     const float *pf = (const float *)((const char *)ep[py] + bo);
@@ -454,8 +565,9 @@ k_sweep_queue(QueueArgs a) {
                         const float hf = __ldg(pf + kTileX * px);
                         const float hb = __ldg(pb + kTileX * px);
                         if constexpr (kF64) {
-                            step_f64<kPrec, false>(cf[py][px], hf, hp[py][px], t.y, dt, slow);
-                            step_f64<kPrec, false>(cb[py][px], hb, hp[py][px], t.y, dt, slow);
+                            const double h64 = hp_of(py, px);
+                            step_f64<kPrec, false>(cf[py][px], hf, h64, dist, dt, slow);
+                            step_f64<kPrec, false>(cb[py][px], hb, h64, dist, dt, slow);
                         } else {
                             step_f32<kPrec, false>(cf[py][px], hf, hp[py][px], t, slow);
                             step_f32<kPrec, false>(cb[py][px], hb, hp[py][px], t, slow);
@@ -496,9 +608,9 @@ k_sweep_queue(QueueArgs a) {
     }
 }
 
-template <int kPrec, int kPx, int kPy, bool kPacked>
+template <int kPrec, int kPx, int kPy, int kVar>
 cudaError_t launch_queue_t(const QueueArgs &a, size_t smem, cudaStream_t s) {
-    auto fn = k_sweep_queue<kPrec, kPx, kPy, kPacked>;
+    auto fn = k_sweep_queue<kPrec, kPx, kPy, kVar>;
     static int blocks_per_sm = -1;
     static size_t configured_smem = 0;
     int dev = 0, sms = 0;
@@ -539,15 +651,17 @@ bool queue_config_valid(const QueueConfig &c) {
 
 QueueConfig default_queue_config() {
     static QueueConfig v = [] {
-        QueueConfig d{2, 1, 0};
+        QueueConfig d{2, 1, 0, 0};
         const char *e = getenv("TVS_SWEEP_SHAPE");
         int x = 0, y = 0;
         if (e && sscanf(e, "%dx%d", &x, &y) == 2) {
-            QueueConfig c{x, y, 0};
+            QueueConfig c{x, y, 0, 0};
             if (queue_config_valid(c)) d.px = x, d.py = y;
         }
         const char *p = getenv("TVS_SWEEP_PACKED");
         if (p) d.packed = atoi(p) != 0;
+        const char *f = getenv("TVS_SWEEP_PREFETCH");
+        if (f) d.prefetch = atoi(f) != 0;
         return d;
     }();
     return v;
@@ -577,22 +691,23 @@ cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, const QueueCon
     if (!f64 && !mix && precision != TVS_PRECISION_EXACT32) return cudaErrorInvalidValue;
     if (!queue_config_valid(c)) return cudaErrorInvalidValue;
     const bool packed = c.packed && !f64 && !mix;
+    const bool pipe = c.prefetch && !packed;
     // ctl + {steps, byte offsets} + FP64 double tables or packed exact-f32 tables (32 B each)
     const bool wide = f64 || mix || packed;
     const size_t smem = sizeof(QueueCtl) +
                         (size_t)a.max_step_cap * (sizeof(float4) + sizeof(long long) + (wide ? 32 : 0));
-#define TVS_Q(X, Y)                                                                    \
-    if (c.px == X && c.py == Y)                                                        \
-        return mix ? launch_queue_t<TVS_PRECISION_MIXED64, X, Y, false>(a, smem, s)    \
-               : f64 ? launch_queue_t<TVS_PRECISION_FP64, X, Y, false>(a, smem, s)     \
-               : packed ? launch_queue_t<TVS_PRECISION_EXACT32, X, Y, true>(a, smem, s) \
-                        : launch_queue_t<TVS_PRECISION_EXACT32, X, Y, false>(a, smem, s);
-    TVS_Q(1, 1) TVS_Q(4, 1) TVS_Q(2, 2) TVS_Q(8, 1)
+#define TVS_Q(X, Y)                                                                         \
+    if (c.px == X && c.py == Y)                                                             \
+        return mix ? (pipe ? launch_queue_t<TVS_PRECISION_MIXED64, X, Y, 2>(a, smem, s)      \
+                           : launch_queue_t<TVS_PRECISION_MIXED64, X, Y, 0>(a, smem, s))     \
+               : f64 ? (pipe ? launch_queue_t<TVS_PRECISION_FP64, X, Y, 2>(a, smem, s)      \
+                             : launch_queue_t<TVS_PRECISION_FP64, X, Y, 0>(a, smem, s))     \
+               : packed ? launch_queue_t<TVS_PRECISION_EXACT32, X, Y, 1>(a, smem, s)        \
+               : pipe ? launch_queue_t<TVS_PRECISION_EXACT32, X, Y, 2>(a, smem, s)          \
+                      : launch_queue_t<TVS_PRECISION_EXACT32, X, Y, 0>(a, smem, s);
+    TVS_Q(1, 1) TVS_Q(2, 1) TVS_Q(4, 1) TVS_Q(2, 2) TVS_Q(8, 1)
 #undef TVS_Q
-    return mix ? launch_queue_t<TVS_PRECISION_MIXED64, 2, 1, false>(a, smem, s)
-           : f64 ? launch_queue_t<TVS_PRECISION_FP64, 2, 1, false>(a, smem, s)
-           : packed ? launch_queue_t<TVS_PRECISION_EXACT32, 2, 1, true>(a, smem, s)
-                    : launch_queue_t<TVS_PRECISION_EXACT32, 2, 1, false>(a, smem, s);
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace tvs

@@ -140,10 +140,11 @@ struct QueueArgs {
     unsigned long long *rechecks;      // MIXED64: FP64 re-decisions (nullable)
 };
 
-// Points of view per thread (columns px 32 apart, rows py 8 apart) and the
-// packed f32x2 arithmetic switch (exact f32 only).
+// Points of view per thread (columns px 32 apart, rows py 8 apart), the
+// packed f32x2 arithmetic switch (exact f32 only) and the elevation prefetch
+// switch (the next step's loads issued before the current step computes).
 struct QueueConfig {
-    int px, py, packed;
+    int px, py, packed, prefetch;
 };
 
 struct PlainArgs {
