@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define TVS_ABI_VERSION 2
+#define TVS_ABI_VERSION 3
 
 /* Status codes.  Negative values are errors; tvs_last_error() has the text. */
 enum tvs_status {
@@ -205,13 +205,17 @@ uint64_t tvs_device_bytes(const tvs_context *ctx);
  * apart times points_y rows 8 apart (1x1, 2x1, 4x1, 2x2, 8x1), i.e. a CTA tile
  * of 32*points_x x 8*points_y points; packed != 0 selects the packed f32x2
  * arithmetic (exact f32 only); prefetch != 0 issues the next step's elevation
- * loads before the current step's arithmetic (not with packed).  Results do
- * not depend on any of them. */
+ * loads before the current step's arithmetic (not with packed).  layout
+ * L in 1..3 (MIXED64 only, with points 4x1) sweeps one direction at a time:
+ * a warp holds LX = 4 << L columns x 32/LX rows of lanes, four points of view
+ * per lane LX columns apart (tiles of 4 LX x 256/LX points); layout 2 is the
+ * MIXED64 default.  Results do not depend on any of them. */
 typedef struct tvs_sweep_config {
     int32_t points_x;
     int32_t points_y;
     int32_t packed;
     int32_t prefetch;
+    int32_t layout;
 } tvs_sweep_config;
 
 int tvs_set_sweep_config(tvs_context *ctx, const tvs_sweep_config *cfg);

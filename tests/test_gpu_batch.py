@@ -79,6 +79,31 @@ def test_sweep_configurations_agree(tvs, synth, shape):
     assert np.array_equal(bits(want), bits(got)) and np.array_equal(bits(wt), bits(gt))
 
 
+@pytest.mark.parametrize("w,h,rows", [(301, 301, None), (311, 197, None), (301, 301, (37, 90))])
+@pytest.mark.parametrize("layout", [0, 1, 2, 3])
+def test_mixed64_layouts_give_fp64_results(tvs, synth, w, h, layout, rows):
+    """Every MIXED64 sweep layout (rows of lanes over both directions, and one
+    direction at a time over 8 x 4, 16 x 2 and 32 x 1 lanes) reproduces the FP64
+    sweep bit for bit, on square and rectangular DEMs and on a row shard."""
+    z = synth.fbm(w, h, 0.8, 11, 0.0, 1200.0)
+    los = int(min(w, h) / 3 * 30.0)
+    kw = dict(observer_height=1.65, height=h, rows=rows)
+    with tvs.Engine(z, w, 30.0, los, precision="fp64", **kw) as e64:
+        want, wt, _ = e64.run()
+    with tvs.Engine(z, w, 30.0, los, precision="mixed64", **kw) as eng:
+        eng.set_sweep_config(4, 1, layout=layout) if layout else eng.set_sweep_config(2, 1)
+        assert eng.sweep_config().layout == layout
+        got, gt, _ = eng.run()
+    assert np.array_equal(bits(want), bits(got)) and np.array_equal(bits(wt), bits(gt))
+
+
+def test_split_layout_is_mixed64_only(tvs, synth):
+    z = synth.config_dem("plain_cpu")
+    with tvs.Engine(z, 301, 30.0, 3000, precision="exact32") as eng:
+        with pytest.raises(tvs.TvsError):
+            eng.set_sweep_config(4, 1, layout=1)
+
+
 @pytest.mark.parametrize("precision", ["mixed64", "fp64"])
 @pytest.mark.parametrize("shape", [(1, 1), (2, 1), (4, 1), (2, 2)])
 def test_prefetch_configurations_agree_wide(tvs, synth, precision, shape):

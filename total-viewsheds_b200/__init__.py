@@ -92,11 +92,12 @@ class SectorStats(ctypes.Structure):
 
 class SweepConfig(ctypes.Structure):
     _fields_ = [("points_x", ctypes.c_int32), ("points_y", ctypes.c_int32),
-                ("packed", ctypes.c_int32), ("prefetch", ctypes.c_int32)]
+                ("packed", ctypes.c_int32), ("prefetch", ctypes.c_int32),
+                ("layout", ctypes.c_int32)]
 
     def __repr__(self):
         return (f"{self.points_x}x{self.points_y}{' packed' if self.packed else ''}"
-                f"{' prefetch' if self.prefetch else ''}")
+                f"{' prefetch' if self.prefetch else ''}{' split' if self.layout == 1 else ''}")
 
 
 SECTOR_CALLBACK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32,
@@ -330,8 +331,8 @@ class Engine:
         self._check(lib().tvs_get_sweep_config(self.ctx, ctypes.byref(c)))
         return c
 
-    def set_sweep_config(self, points_x, points_y, packed=False, prefetch=False):
-        c = SweepConfig(points_x, points_y, 1 if packed else 0, 1 if prefetch else 0)
+    def set_sweep_config(self, points_x, points_y, packed=False, prefetch=False, layout=0):
+        c = SweepConfig(points_x, points_y, 1 if packed else 0, 1 if prefetch else 0, layout)
         self._check(lib().tvs_set_sweep_config(self.ctx, ctypes.byref(c)))
 
     def autotune(self, sample_sectors=4):
@@ -408,8 +409,8 @@ class Batch:
         self._check(lib().tvs_batch_autotune(self.b, sample_sectors, ctypes.byref(c)))
         return c
 
-    def set_sweep_config(self, points_x, points_y, packed=False, prefetch=False):
-        c = SweepConfig(points_x, points_y, 1 if packed else 0, 1 if prefetch else 0)
+    def set_sweep_config(self, points_x, points_y, packed=False, prefetch=False, layout=0):
+        c = SweepConfig(points_x, points_y, 1 if packed else 0, 1 if prefetch else 0, layout)
         self._check(lib().tvs_batch_set_sweep_config(self.b, ctypes.byref(c)))
 
     def run(self):

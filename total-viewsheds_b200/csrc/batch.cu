@@ -34,7 +34,7 @@ struct tvs_batch {
     unsigned long long *d_rechecks = nullptr;
     uint32_t max_step_cap = 0;
     uint32_t tiles_per_sector = 0;
-    tvs::QueueConfig cfg{0, 0, 0, 0};
+    tvs::QueueConfig cfg{0, 0, 0, 0, 0};
     bool dems_uploaded = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -176,7 +176,7 @@ int tvs_batch_create(const tvs_params *params, const float *const *elevations, u
         bail(e == cudaErrorMemoryAllocation ? TVS_ERR_OUT_OF_MEMORY : TVS_ERR_CUDA);
         return bfail(nullptr, e == cudaErrorMemoryAllocation ? TVS_ERR_OUT_OF_MEMORY : TVS_ERR_CUDA, m);
     }
-    b->cfg = tvs::default_queue_config();
+    b->cfg = tvs::default_queue_config((int)b->precision);
     int rc = upload_dems(b);
     if (rc) {
         std::string m = b->err;
@@ -213,11 +213,13 @@ int tvs_batch_geometry(const tvs_batch *b, uint32_t dem, tvs_geometry *out) {
 
 int tvs_batch_set_sweep_config(tvs_batch *b, const tvs_sweep_config *cfg) {
     if (!b || !cfg) return TVS_ERR_INVALID_ARGUMENT;
-    tvs::QueueConfig c{cfg->points_x, cfg->points_y, cfg->packed != 0, cfg->prefetch != 0};
+    tvs::QueueConfig c{cfg->points_x, cfg->points_y, cfg->packed != 0, cfg->prefetch != 0, cfg->layout};
     if (!tvs::queue_config_valid(c))
         return bfail(b, TVS_ERR_INVALID_ARGUMENT, "unsupported points-per-thread shape");
+    if (c.layout != 0 && b->precision != TVS_PRECISION_MIXED64)
+        return bfail(b, TVS_ERR_INVALID_ARGUMENT, "sweep layouts 1-3 are MIXED64 only");
     if (c.px != b->cfg.px || c.py != b->cfg.py || c.packed != b->cfg.packed ||
-        c.prefetch != b->cfg.prefetch) {
+        c.prefetch != b->cfg.prefetch || c.layout != b->cfg.layout) {
         b->cfg = c;
         b->dems_uploaded = false;
         drop_graph(b);
@@ -231,6 +233,7 @@ int tvs_batch_get_sweep_config(const tvs_batch *b, tvs_sweep_config *cfg) {
     cfg->points_y = b->cfg.py;
     cfg->packed = b->cfg.packed;
     cfg->prefetch = b->cfg.prefetch;
+    cfg->layout = b->cfg.layout;
     return TVS_OK;
 }
 
@@ -240,9 +243,12 @@ int tvs_batch_autotune(tvs_batch *b, uint32_t sample_sectors, tvs_sweep_config *
         return bfail(b, TVS_ERR_INVALID_ARGUMENT, "sample_sectors must be in [1, 180]");
     TVS_BCUDA(b, cudaSetDevice(b->device));
     const bool exact = b->precision == TVS_PRECISION_EXACT32;
-    const tvs::QueueConfig cands[] = {{1, 1, 0, 0}, {2, 1, 0, 0}, {4, 1, 0, 0}, {2, 2, 0, 0},
-                                      {2, 1, 1, 0}, {4, 1, 1, 0}, {1, 1, 0, 1}, {2, 1, 0, 1},
-                                      {4, 1, 0, 1}, {2, 2, 0, 1}};
+    const bool mix = b->precision == TVS_PRECISION_MIXED64;
+    const tvs::QueueConfig cands[] = {{1, 1, 0, 0, 0}, {2, 1, 0, 0, 0}, {4, 1, 0, 0, 0},
+                                      {2, 2, 0, 0, 0}, {2, 1, 1, 0, 0}, {4, 1, 1, 0, 0},
+                                      {1, 1, 0, 1, 0}, {2, 1, 0, 1, 0}, {4, 1, 0, 1, 0},
+                                      {2, 2, 0, 1, 0}, {4, 1, 0, 0, 1}, {4, 1, 0, 0, 2},
+                                      {4, 1, 0, 0, 3}};
     cudaEvent_t t0, t1;
     TVS_BCUDA(b, cudaEventCreate(&t0));
     TVS_BCUDA(b, cudaEventCreate(&t1));
@@ -250,8 +256,8 @@ int tvs_batch_autotune(tvs_batch *b, uint32_t sample_sectors, tvs_sweep_config *
     tvs::QueueConfig best_cfg = b->cfg;
     int rc = TVS_OK;
     for (const tvs::QueueConfig &c : cands) {
-        if (c.packed && !exact) continue;
-        tvs_sweep_config sc{c.px, c.py, c.packed, c.prefetch};
+        if ((c.packed && !exact) || (c.layout != 0 && !mix)) continue;
+        tvs_sweep_config sc{c.px, c.py, c.packed, c.prefetch, c.layout};
         if ((rc = tvs_batch_set_sweep_config(b, &sc))) break;
         float ms = 0.0f;
         for (int rep = 0; rep < 2 && rc == TVS_OK; rep++) {  // the first run warms up
@@ -271,7 +277,7 @@ int tvs_batch_autotune(tvs_batch *b, uint32_t sample_sectors, tvs_sweep_config *
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     if (rc) return rc;
-    tvs_sweep_config sc{best_cfg.px, best_cfg.py, best_cfg.packed, best_cfg.prefetch};
+    tvs_sweep_config sc{best_cfg.px, best_cfg.py, best_cfg.packed, best_cfg.prefetch, best_cfg.layout};
     rc = tvs_batch_set_sweep_config(b, &sc);
     if (rc == TVS_OK && chosen) *chosen = sc;
     return rc;

@@ -294,7 +294,7 @@ tvs::QueueDem queue_dem(const tvs_context *c) {
 
 int upload_queue_dem(tvs_context *c) {
     const tvs::QueueConfig &q = c->qcfg, &u = c->qcfg_uploaded;
-    if (q.px == u.px && q.py == u.py && q.packed == u.packed) return TVS_OK;
+    if (q.px == u.px && q.py == u.py && q.layout == u.layout) return TVS_OK;
     tvs::QueueDem d = queue_dem(c);
     uint32_t done_total = 0;
     tvs::queue_tile(&d, 1, q, &c->q_tiles_per_sector, &done_total);
@@ -521,7 +521,7 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
     }
     c->step_cap = (g.band_steps_filled + 2 + 3) & ~3u;
     c->done_cap = tvs::queue_tiles_bound(g.tvs_width, re - rb);
-    c->qcfg = tvs::default_queue_config();
+    c->qcfg = tvs::default_queue_config((int)c->p.precision);
     auto bail = [&](cudaError_t e, const char *what) {
         std::string m = std::string(what) + ": " + cudaGetErrorString(e);
         int code = e == cudaErrorMemoryAllocation ? TVS_ERR_OUT_OF_MEMORY : TVS_ERR_CUDA;
@@ -828,9 +828,11 @@ const float *tvs_device_cumulative(const tvs_context *ctx) { return ctx ? ctx->d
 
 int tvs_set_sweep_config(tvs_context *ctx, const tvs_sweep_config *cfg) {
     if (!ctx || !cfg) return TVS_ERR_INVALID_ARGUMENT;
-    tvs::QueueConfig c{cfg->points_x, cfg->points_y, cfg->packed != 0, cfg->prefetch != 0};
+    tvs::QueueConfig c{cfg->points_x, cfg->points_y, cfg->packed != 0, cfg->prefetch != 0, cfg->layout};
     if (!tvs::queue_config_valid(c))
         return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "unsupported points-per-thread shape");
+    if (c.layout != 0 && ctx->p.precision != TVS_PRECISION_MIXED64)
+        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "sweep layouts 1-3 are MIXED64 only");
     ctx->qcfg = c;
     return TVS_OK;
 }
@@ -841,6 +843,7 @@ int tvs_get_sweep_config(const tvs_context *ctx, tvs_sweep_config *cfg) {
     cfg->points_y = ctx->qcfg.py;
     cfg->packed = ctx->qcfg.packed;
     cfg->prefetch = ctx->qcfg.prefetch;
+    cfg->layout = ctx->qcfg.layout;
     return TVS_OK;
 }
 
@@ -850,9 +853,12 @@ int tvs_autotune(tvs_context *ctx, uint32_t sample_sectors, tvs_sweep_config *ch
         return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "sample_sectors must be in [1, 180]");
     TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
     const bool exact = ctx->p.precision == TVS_PRECISION_EXACT32;
-    const tvs::QueueConfig cands[] = {{1, 1, 0, 0}, {2, 1, 0, 0}, {4, 1, 0, 0}, {2, 2, 0, 0},
-                                      {2, 1, 1, 0}, {4, 1, 1, 0}, {1, 1, 0, 1}, {2, 1, 0, 1},
-                                      {4, 1, 0, 1}, {2, 2, 0, 1}};
+    const bool mix = ctx->p.precision == TVS_PRECISION_MIXED64;
+    const tvs::QueueConfig cands[] = {{1, 1, 0, 0, 0}, {2, 1, 0, 0, 0}, {4, 1, 0, 0, 0},
+                                      {2, 2, 0, 0, 0}, {2, 1, 1, 0, 0}, {4, 1, 1, 0, 0},
+                                      {1, 1, 0, 1, 0}, {2, 1, 0, 1, 0}, {4, 1, 0, 1, 0},
+                                      {2, 2, 0, 1, 0}, {4, 1, 0, 0, 1}, {4, 1, 0, 0, 2},
+                                      {4, 1, 0, 0, 3}};
     cudaEvent_t t0, t1;
     TVS_CUDA(ctx, cudaEventCreate(&t0));
     TVS_CUDA(ctx, cudaEventCreate(&t1));
@@ -861,7 +867,7 @@ int tvs_autotune(tvs_context *ctx, uint32_t sample_sectors, tvs_sweep_config *ch
     int rc = enqueue_shape(ctx, 0, sample_sectors);
     for (const tvs::QueueConfig &c : cands) {
         if (rc) break;
-        if (c.packed && !exact) continue;
+        if ((c.packed && !exact) || (c.layout != 0 && !mix)) continue;
         ctx->qcfg = c;
         float ms = 0.0f;
         for (int rep = 0; rep < 2 && rc == TVS_OK; rep++) {  // the first run warms up

@@ -161,22 +161,160 @@ __device__ __forceinline__ void step_f64(Chain<kPrec> &c, float h, double hp, fl
 #ifndef TVS_MIX_MIN_BLOCKS
 #define TVS_MIX_MIN_BLOCKS 4
 #endif
-template <int kPrec, int kPx, int kPy>
+template <int kPrec, int kPx, int kPy, int kVar>
 constexpr int queue_min_blocks() {
     return kPrec != TVS_PRECISION_MIXED64 ? 1
+           : kVar >= 3                    ? TVS_MIX_MIN_BLOCKS
            : kPx * kPy <= 2               ? TVS_MIX_MIN_BLOCKS
            : kPx * kPy == 4               ? 2
                                           : 1;
 }
 
+// MIXED64, one direction at a time.  A warp holds LX columns x 32/LX rows of
+// lanes and each lane four points of view LX columns apart; the 8 warps of a
+// CTA stack in rows: a tile is 4 LX x 256/LX points (layout 1: LX = 8, 32 x 32;
+// layout 2: LX = 16, 64 x 16; layout 3: LX = 32, 128 x 8).  A lane sweeps its
+// four forward chains over all steps, then its four backward chains.  Chains
+// of one direction over a compact patch of points of view see their running
+// maximum rise at nearly the same steps, so a warp enters the classification
+// at fewer steps than when it mixes directions; narrower patches gain more
+// there and pay more L1 sectors per load (rows of LX * 4 bytes).
+constexpr int kSplitCols = 4;  // points of view per lane
+__host__ __device__ constexpr int split_lx(int layout) { return 4 << layout; }
+__host__ __device__ constexpr int split_tile_w(int layout) { return kSplitCols * split_lx(layout); }
+__host__ __device__ constexpr int split_tile_h(int layout) { return kTileY * (32 / split_lx(layout)); }
+
+template <int LX, class Wait>
+__device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const QueueDem &D, uint32_t bx,
+                                                 uint32_t by, uint32_t n, uint32_t n_fast,
+                                                 const float4 *s_steps, const long long *s_boff,
+                                                 const double4 *s_dtab, double *s_fwd, Wait &&wait_prev) {
+    constexpr int K = kSplitCols, LY = 32 / LX;
+    const uint32_t lx = threadIdx.x % LX, ly = threadIdx.x / LX;
+    const uint32_t tx = bx * (K * LX) + lx;  // columns tx + LX k
+    const uint32_t ty = D.row_begin + by * (kTileY * LY) + threadIdx.y * LY + ly;
+    // rows past the grid are clamped, columns past it read padding; both are discarded
+    const float *ep = D.elev + (int64_t)(min(ty, D.row_end - 1) + D.los) * D.width + tx + D.los;
+    float hp32[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) hp32[k] = __fadd_rn(__ldg(ep + LX * k), D.observer_height);
+    auto hp64 = [&](int k) -> double {
+        return __dadd_rn((double)__ldg(ep + LX * k), (double)D.observer_height);
+    };
+    // forward surfaces wait in shared memory (s_fwd[k * kThreads + tid]) while
+    // the backward chains run
+    const uint32_t tid = threadIdx.y * kTileX + threadIdx.x;
+    double sb[K];
+    // one direction's sweep; DIR is a compile-time 0 (forward) or 1 (backward)
+    auto pass = [&](auto DIR) {
+        constexpr int dir = decltype(DIR)::value;
+        auto at = [&](uint32_t step) -> const float * {
+            const long long b = s_boff[step];
+            return (const float *)((const char *)ep + (dir ? -b : b));
+        };
+        auto exact_angle = [&](int k, uint32_t step) -> double {
+            const double ek = __dsub_rn((double)__ldg(at(step) + LX * k), hp64(k));
+            const double4 dk = s_dtab[step];
+            return __dsub_rn(div_table64(ek, dk.x, dk.w), dk.y);
+        };
+        auto max64 = [&](int k, int32_t j) -> double {
+            return j < 0 ? -2000.0 : exact_angle(k, (uint32_t)j);
+        };
+        Chain<TVS_PRECISION_MIXED64> c[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) c[k].init();
+        uint32_t i = 0;
+        for (; i < n_fast; i++) {
+            const float4 t = s_steps[i];
+            const float *pe = at(i);
+            // filter (see the row layout): estimate + g >= m32 - gm
+            float e[K];
+            bool hit = false;
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                e[k] = __fsub_rn(__ldg(pe + LX * k), hp32[k]);
+                hit |= __fmaf_rn(e[k], t.x, t.y) >= c[k].lo;
+            }
+            if (!__any_sync(0xffffffffu, hit)) continue;
+            const double w64 = s_dtab[i].z;
+            float ah[K], dd[K];
+            bool any_amb = false;
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                ah[k] = __fmaf_rn(e[k], t.x, t.z);
+                dd[k] = __fsub_rn(ah[k], c[k].m32);
+                const bool am = fabsf(dd[k]) <= __fadd_rn(t.w, c[k].gm);
+                if (!am && dd[k] > 0.0f) {  // surely visible
+                    c[k].set_max32(ah[k], t.w);
+                    c[k].j = (int32_t)i;
+                    c[k].s = __dadd_rn(c[k].s, w64);
+                }
+                any_amb |= am;
+            }
+            if (__any_sync(0xffffffffu, any_amb)) {
+                // a chain surely visible at this step has j == i; every other
+                // chain still has the state it was tested with
+#pragma unroll
+                for (int k = 0; k < K; k++) {
+                    if (c[k].j == (int32_t)i) continue;
+                    if (!(fabsf(dd[k]) <= __fadd_rn(t.w, c[k].gm))) continue;
+                    if (a.rechecks) atomicAdd(a.rechecks, 1ull);
+                    const double a64 = exact_angle(k, i);
+                    if (a64 > max64(k, c[k].j)) {
+                        c[k].j = (int32_t)i;
+                        c[k].set_max32(ah[k], t.w);
+                        c[k].s = __dadd_rn(c[k].s, w64);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++) c[k].m = max64(k, c[k].j);
+        // the steps past the table-division domain (zero distances), IEEE division
+        for (; i < n; i++) {
+            const double4 dt = s_dtab[i];
+            const float dist = (float)dt.w;
+            const int slow = !(dist >= 0x1p-20f && dist <= 0x1p20f);
+            const float *pe = at(i);
+#pragma unroll
+            for (int k = 0; k < K; k++)
+                step_f64<TVS_PRECISION_MIXED64, false>(c[k], __ldg(pe + LX * k), hp64(k), dist, dt, slow);
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            if (dir == 0) s_fwd[k * kThreads + tid] = c[k].s;
+            else sb[k] = c[k].s;
+        }
+    };
+    pass(std::integral_constant<int, 0>{});
+    pass(std::integral_constant<int, 1>{});
+    const bool write = wait_prev();  // every thread of the CTA reaches it
+    if (!write || ty >= D.row_end) return;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        const uint32_t col = tx + LX * k;
+        if (col >= D.tvs_width) continue;
+        const uint64_t p = (uint64_t)ty * D.tvs_width + col;
+        // forward surface first (kernel.rs:254), in L2 like the row layout
+        const double cum = __dadd_rn(__dadd_rn(__ldcg(D.cumulative64 + p), s_fwd[k * kThreads + tid]), sb[k]);
+        __stcg(D.cumulative64 + p, cum);
+        const float c32 = __double2float_rn(cum);
+        __stcg(D.cumulative + p, c32);
+        if (D.total) __stcg(D.total + p, __fadd_rn(__ldcg(D.total + p), c32));
+    }
+}
+
 // kVar: 0 scalar, 1 packed f32x2 (exact f32 only), 2 scalar with the next
-// step's elevations loaded while the current step computes.
+// step's elevations loaded while the current step computes, 3-5 the MIXED64
+// direction-split layouts 1-3 above (kPx, kPy unused).
 template <int kPrec, int kPx, int kPy, int kVar>
-__global__ void __launch_bounds__(kThreads, (queue_min_blocks<kPrec, kPx, kPy>()))
+__global__ void __launch_bounds__(kThreads, (queue_min_blocks<kPrec, kPx, kPy, kVar>()))
 k_sweep_queue(QueueArgs a) {
     constexpr bool kPacked = kVar == 1;
     constexpr bool kPipe = kVar == 2;
+    constexpr bool kSplit = kVar >= 3;
     constexpr bool kMix = kPrec == TVS_PRECISION_MIXED64;
+    static_assert(!kSplit || kMix, "the direction-split layout is MIXED64 only");
     constexpr bool kF64 = kPrec == TVS_PRECISION_FP64 || kMix;  // FP64 tables and surfaces
     extern __shared__ __align__(16) unsigned char smem[];
     QueueCtl &ctl = *reinterpret_cast<QueueCtl *>(smem);
@@ -256,7 +394,11 @@ k_sweep_queue(QueueArgs a) {
                 ctl.n_fast = h->n_fast;
             }
         }
-        // This tile's previous sector must be complete (bounded wait).
+        __syncthreads();  // the staged tables
+        // The tile's previous sector must be complete before this sector's
+        // surfaces are added (bounded wait).  It is awaited after the sweep,
+        // by which time it has almost always finished.
+        auto wait_prev = [&]() -> bool {
         if (tid == 0) {
             ctl.wait_status = TVS_OK;
             if (s > 0) {
@@ -276,12 +418,18 @@ k_sweep_queue(QueueArgs a) {
             }
         }
         __syncthreads();
-        const bool run = ctl.sector_status == TVS_OK && ctl.wait_status == TVS_OK;
+        return ctl.wait_status == TVS_OK;
+        };
+        const bool run = ctl.sector_status == TVS_OK;
         const uint32_t n = ctl.n_steps, n_fast = ctl.n_fast;
         const uint32_t bx = tile % D.tiles_x, by = tile / D.tiles_x;
         const uint32_t tx0 = bx * (kTileX * kPx) + threadIdx.x;
         const uint32_t ty0 = D.row_begin + by * (kTileY * kPy) + threadIdx.y;
-        if (run) {
+        if constexpr (kSplit) {
+            if (run)
+                sweep_tile_split<split_lx(kVar - 2)>(a, D, bx, by, n, n_fast, s_steps, s_boff, s_dtab,
+                                 reinterpret_cast<double *>(s_dtab + a.max_step_cap), wait_prev);
+        } else if (run) {
             const float *ep[kPy];
             using HP = typename std::conditional<kF64, double, float>::type;
             HP hp[kPy][kPx];
@@ -575,10 +723,11 @@ k_sweep_queue(QueueArgs a) {
                     }
                 }
             }
+            const bool write = wait_prev();
 #pragma unroll
             for (int py = 0; py < kPy; py++) {
                 const uint32_t ty = ty0 + py * kTileY;
-                if (ty >= D.row_end) continue;
+                if (!write || ty >= D.row_end) continue;
 #pragma unroll
                 for (int px = 0; px < kPx; px++) {
                     const uint32_t tx = tx0 + kTileX * px;
@@ -643,19 +792,22 @@ uint32_t queue_tiles_bound(uint32_t tvs_width, uint32_t rows) {
 }
 
 bool queue_config_valid(const QueueConfig &c) {
+    if (c.layout >= 1 && c.layout <= 3)
+        return c.px == kSplitCols && c.py == 1 && !c.packed && !c.prefetch;
+    if (c.layout != 0) return false;
     const int ok[][2] = {{1, 1}, {2, 1}, {4, 1}, {2, 2}, {8, 1}};
     for (const auto &k : ok)
         if (k[0] == c.px && k[1] == c.py) return true;
     return false;
 }
 
-QueueConfig default_queue_config() {
+QueueConfig default_queue_config(int precision) {
     static QueueConfig v = [] {
-        QueueConfig d{2, 1, 0, 0};
+        QueueConfig d{2, 1, 0, 0, 0};
         const char *e = getenv("TVS_SWEEP_SHAPE");
         int x = 0, y = 0;
         if (e && sscanf(e, "%dx%d", &x, &y) == 2) {
-            QueueConfig c{x, y, 0, 0};
+            QueueConfig c{x, y, 0, 0, 0};
             if (queue_config_valid(c)) d.px = x, d.py = y;
         }
         const char *p = getenv("TVS_SWEEP_PACKED");
@@ -664,6 +816,14 @@ QueueConfig default_queue_config() {
         if (f) d.prefetch = atoi(f) != 0;
         return d;
     }();
+    // MIXED64 defaults to layout 2 (the fastest of the four on one B200 at
+    // 2401^2 and 3601^2); TVS_SWEEP_LAYOUT overrides it
+    static const int split = [] {
+        const char *l = getenv("TVS_SWEEP_LAYOUT");
+        return l ? atoi(l) : 2;
+    }();
+    if (precision == TVS_PRECISION_MIXED64 && split >= 1 && split <= 3)
+        return QueueConfig{kSplitCols, 1, 0, 0, split};
     return v;
 }
 
@@ -673,8 +833,10 @@ void queue_tile(QueueDem *dems, uint32_t n_dems, const QueueConfig &c, uint32_t 
     for (uint32_t i = 0; i < n_dems; i++) {
         QueueDem &d = dems[i];
         const uint32_t rows = d.row_end - d.row_begin;
-        d.tiles_x = (d.tvs_width + kTileX * c.px - 1) / (kTileX * c.px);
-        d.tiles_y = (rows + kTileY * c.py - 1) / (kTileY * c.py);
+        const uint32_t tw = c.layout ? split_tile_w(c.layout) : kTileX * c.px;
+        const uint32_t th = c.layout ? split_tile_h(c.layout) : kTileY * c.py;
+        d.tiles_x = (d.tvs_width + tw - 1) / tw;
+        d.tiles_y = (rows + th - 1) / th;
         d.tile_base = base;
         d.done_base = base;
         base += d.tiles_x * d.tiles_y;
@@ -690,12 +852,15 @@ cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, const QueueCon
     const bool f64 = precision == TVS_PRECISION_FP64;
     if (!f64 && !mix && precision != TVS_PRECISION_EXACT32) return cudaErrorInvalidValue;
     if (!queue_config_valid(c)) return cudaErrorInvalidValue;
+    if (c.layout != 0 && !mix) return cudaErrorInvalidValue;
     const bool packed = c.packed && !f64 && !mix;
     const bool pipe = c.prefetch && !packed;
     // ctl + {steps, byte offsets} + FP64 double tables or packed exact-f32 tables (32 B each)
     const bool wide = f64 || mix || packed;
+    // (+ the forward surfaces of the direction-split layout)
     const size_t smem = sizeof(QueueCtl) +
-                        (size_t)a.max_step_cap * (sizeof(float4) + sizeof(long long) + (wide ? 32 : 0));
+                        (size_t)a.max_step_cap * (sizeof(float4) + sizeof(long long) + (wide ? 32 : 0)) +
+                        (c.layout ? (size_t)kThreads * kSplitCols * sizeof(double) : 0);
 #define TVS_Q(X, Y)                                                                         \
     if (c.px == X && c.py == Y)                                                             \
         return mix ? (pipe ? launch_queue_t<TVS_PRECISION_MIXED64, X, Y, 2>(a, smem, s)      \
@@ -705,6 +870,9 @@ cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, const QueueCon
                : packed ? launch_queue_t<TVS_PRECISION_EXACT32, X, Y, 1>(a, smem, s)        \
                : pipe ? launch_queue_t<TVS_PRECISION_EXACT32, X, Y, 2>(a, smem, s)          \
                       : launch_queue_t<TVS_PRECISION_EXACT32, X, Y, 0>(a, smem, s);
+    if (c.layout == 1) return launch_queue_t<TVS_PRECISION_MIXED64, 1, 1, 3>(a, smem, s);
+    if (c.layout == 2) return launch_queue_t<TVS_PRECISION_MIXED64, 1, 1, 4>(a, smem, s);
+    if (c.layout == 3) return launch_queue_t<TVS_PRECISION_MIXED64, 1, 1, 5>(a, smem, s);
     TVS_Q(1, 1) TVS_Q(2, 1) TVS_Q(4, 1) TVS_Q(2, 2) TVS_Q(8, 1)
 #undef TVS_Q
     return cudaErrorInvalidValue;

@@ -34,8 +34,8 @@ struct tvs_context {
     float *d_hmax = nullptr;  // max |elevation| + |observer height| (MIXED64 window)
     unsigned long long *d_rechecks = nullptr;  // MIXED64 FP64 re-decisions
     tvs::QueueDem *d_qdem = nullptr;           // this context as a one-DEM queue
-    tvs::QueueConfig qcfg{0, 0, 0, 0};            // sweep configuration (autotuned or default)
-    tvs::QueueConfig qcfg_uploaded{0, 0, 0, 0};   // the tiling currently in d_qdem
+    tvs::QueueConfig qcfg{0, 0, 0, 0, 0};            // sweep configuration (autotuned or default)
+    tvs::QueueConfig qcfg_uploaded{0, 0, 0, 0, 0};   // the tiling currently in d_qdem
     uint32_t q_tiles_per_sector = 0;
     int32_t *d_deltas = nullptr;
     float *d_dists = nullptr;

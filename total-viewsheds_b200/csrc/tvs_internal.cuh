@@ -141,10 +141,12 @@ struct QueueArgs {
 };
 
 // Points of view per thread (columns px 32 apart, rows py 8 apart), the
-// packed f32x2 arithmetic switch (exact f32 only) and the elevation prefetch
-// switch (the next step's loads issued before the current step computes).
+// packed f32x2 arithmetic switch (exact f32 only), the elevation prefetch
+// switch (the next step's loads issued before the current step computes) and
+// the layout: 0 rows of 32 lanes sweeping both directions together, 1 the
+// MIXED64 direction-split layout (8 x 4 lanes, px = 4 points 8 columns apart).
 struct QueueConfig {
-    int px, py, packed, prefetch;
+    int px, py, packed, prefetch, layout;
 };
 
 struct PlainArgs {
@@ -191,7 +193,7 @@ cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, const QueueCon
                                cudaStream_t s);
 uint32_t queue_tiles_bound(uint32_t tvs_width, uint32_t rows);
 bool queue_config_valid(const QueueConfig &c);
-QueueConfig default_queue_config();
+QueueConfig default_queue_config(int precision);
 // Sets tiles_x/tiles_y/tile_base/done_base of every DEM for the configuration.
 void queue_tile(QueueDem *dems, uint32_t n_dems, const QueueConfig &c, uint32_t *tiles_per_sector,
                 uint32_t *done_total);
