@@ -206,7 +206,8 @@ uint64_t tvs_device_bytes(const tvs_context *ctx);
  * of 32*points_x x 8*points_y points; packed != 0 selects the packed f32x2
  * arithmetic (exact f32 only); prefetch != 0 issues the next step's elevation
  * loads before the current step's arithmetic (not with packed).  layout
- * L in 1..3 (MIXED64 only, with points 4x1) sweeps one direction at a time:
+ * L in 1..3 (MIXED64 and EXACT32, with points 4x1) sweeps one direction at a
+ * time, evaluating angles exactly only where a warp's filter passes:
  * a warp holds LX = 4 << L columns x 32/LX rows of lanes, four points of view
  * per lane LX columns apart (tiles of 4 LX x 256/LX points); layout 2 is the
  * MIXED64 default.  Results do not depend on any of them. */

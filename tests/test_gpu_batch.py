@@ -81,25 +81,30 @@ def test_sweep_configurations_agree(tvs, synth, shape):
 
 @pytest.mark.parametrize("w,h,rows", [(301, 301, None), (311, 197, None), (301, 301, (37, 90))])
 @pytest.mark.parametrize("layout", [0, 1, 2, 3])
-def test_mixed64_layouts_give_fp64_results(tvs, synth, w, h, layout, rows):
-    """Every MIXED64 sweep layout (rows of lanes over both directions, and one
-    direction at a time over 8 x 4, 16 x 2 and 32 x 1 lanes) reproduces the FP64
-    sweep bit for bit, on square and rectangular DEMs and on a row shard."""
+@pytest.mark.parametrize("precision,reference", [("mixed64", "fp64"), ("exact32", "exact32")])
+def test_split_layouts_agree(tvs, synth, w, h, layout, rows, precision, reference):
+    """Every sweep layout (rows of lanes over both directions, and one direction
+    at a time over 8 x 4, 16 x 2 and 32 x 1 lanes) gives the reference sweep bit
+    for bit (MIXED64: the FP64 sweep; exact f32: the row layout, itself checked
+    against the oracle elsewhere), on square and rectangular DEMs and on a row
+    shard."""
     z = synth.fbm(w, h, 0.8, 11, 0.0, 1200.0)
     los = int(min(w, h) / 3 * 30.0)
     kw = dict(observer_height=1.65, height=h, rows=rows)
-    with tvs.Engine(z, w, 30.0, los, precision="fp64", **kw) as e64:
+    with tvs.Engine(z, w, 30.0, los, precision=reference, **kw) as e64:
+        if reference == "exact32":
+            e64.set_sweep_config(2, 1)
         want, wt, _ = e64.run()
-    with tvs.Engine(z, w, 30.0, los, precision="mixed64", **kw) as eng:
+    with tvs.Engine(z, w, 30.0, los, precision=precision, **kw) as eng:
         eng.set_sweep_config(4, 1, layout=layout) if layout else eng.set_sweep_config(2, 1)
         assert eng.sweep_config().layout == layout
         got, gt, _ = eng.run()
     assert np.array_equal(bits(want), bits(got)) and np.array_equal(bits(wt), bits(gt))
 
 
-def test_split_layout_is_mixed64_only(tvs, synth):
+def test_split_layout_is_not_for_fp64(tvs, synth):
     z = synth.config_dem("plain_cpu")
-    with tvs.Engine(z, 301, 30.0, 3000, precision="exact32") as eng:
+    with tvs.Engine(z, 301, 30.0, 3000, precision="fp64") as eng:
         with pytest.raises(tvs.TvsError):
             eng.set_sweep_config(4, 1, layout=1)
 
@@ -127,3 +132,28 @@ def test_engine_autotune(tvs, synth):
         assert eng.sweep_config().points_x == cfg.points_x
         got, _, _ = eng.run()
     assert np.array_equal(bits(want), bits(got))
+
+
+@pytest.mark.parametrize("kind", ["terraces", "steep"])
+@pytest.mark.parametrize("layout", [1, 2, 3])
+@pytest.mark.parametrize("precision,reference", [("mixed64", "fp64"), ("exact32", "exact32")])
+def test_split_layouts_on_hard_terrain(tvs, synth, kind, layout, precision, reference):
+    """The filtered layouts on terrain that stresses the filter: terraces (many
+    equal elevations, so equal and near-equal angles) and 1 m cells with 6 km of
+    relief (angles in the thousands, near the initial maximum of -2000)."""
+    w = 161
+    z = synth.fbm(w, w, 0.7, 5, 0.0, 1500.0)
+    scale, los = 30.0, 1500
+    if kind == "terraces":
+        z = (np.round(z / 50.0) * 50.0).astype(np.float32)
+    else:
+        z = synth.fbm(w, w, 0.5, 6, 0.0, 6000.0)
+        scale, los = 1.0, 50
+    with tvs.Engine(z, w, scale, los, precision=reference, observer_height=1.65) as ref:
+        if reference == "exact32":
+            ref.set_sweep_config(2, 1)
+        want, wt, _ = ref.run()
+    with tvs.Engine(z, w, scale, los, precision=precision, observer_height=1.65) as eng:
+        eng.set_sweep_config(4, 1, layout=layout)
+        got, gt, _ = eng.run()
+    assert np.array_equal(bits(want), bits(got)) and np.array_equal(bits(wt), bits(gt))

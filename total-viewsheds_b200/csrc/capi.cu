@@ -831,8 +831,8 @@ int tvs_set_sweep_config(tvs_context *ctx, const tvs_sweep_config *cfg) {
     tvs::QueueConfig c{cfg->points_x, cfg->points_y, cfg->packed != 0, cfg->prefetch != 0, cfg->layout};
     if (!tvs::queue_config_valid(c))
         return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "unsupported points-per-thread shape");
-    if (c.layout != 0 && ctx->p.precision != TVS_PRECISION_MIXED64)
-        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "sweep layouts 1-3 are MIXED64 only");
+    if (c.layout != 0 && ctx->p.precision == TVS_PRECISION_FP64)
+        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "sweep layouts 1-3 are not available for FP64");
     ctx->qcfg = c;
     return TVS_OK;
 }
@@ -853,7 +853,7 @@ int tvs_autotune(tvs_context *ctx, uint32_t sample_sectors, tvs_sweep_config *ch
         return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "sample_sectors must be in [1, 180]");
     TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
     const bool exact = ctx->p.precision == TVS_PRECISION_EXACT32;
-    const bool mix = ctx->p.precision == TVS_PRECISION_MIXED64;
+    const bool f64 = ctx->p.precision == TVS_PRECISION_FP64;
     const tvs::QueueConfig cands[] = {{1, 1, 0, 0, 0}, {2, 1, 0, 0, 0}, {4, 1, 0, 0, 0},
                                       {2, 2, 0, 0, 0}, {2, 1, 1, 0, 0}, {4, 1, 1, 0, 0},
                                       {1, 1, 0, 1, 0}, {2, 1, 0, 1, 0}, {4, 1, 0, 1, 0},
@@ -867,7 +867,7 @@ int tvs_autotune(tvs_context *ctx, uint32_t sample_sectors, tvs_sweep_config *ch
     int rc = enqueue_shape(ctx, 0, sample_sectors);
     for (const tvs::QueueConfig &c : cands) {
         if (rc) break;
-        if ((c.packed && !exact) || (c.layout != 0 && !mix)) continue;
+        if ((c.packed && !exact) || (c.layout != 0 && f64)) continue;
         ctx->qcfg = c;
         float ms = 0.0f;
         for (int rep = 0; rep < 2 && rc == TVS_OK; rep++) {  // the first run warms up

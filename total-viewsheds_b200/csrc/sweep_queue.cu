@@ -123,7 +123,15 @@ template <> struct Chain<TVS_PRECISION_MIXED64> {
     double m, s;
     float m32, gm, lo;
     int32_t j;
-    __device__ void init() { m = -2000.0; s = 0.0; m32 = -2000.0f; gm = 0.0f; lo = -2000.0f; j = -1; }
+    // the initial maximum carries the |m| 2^-19 part of the window like any other
+    __device__ void init() {
+        m = -2000.0;
+        s = 0.0;
+        m32 = -2000.0f;
+        gm = 2000.0f * 0x1p-19f;
+        lo = __fsub_rn(m32, gm);
+        j = -1;
+    }
     __device__ void set_max32(float ah, float g) {
         m32 = ah;
         gm = __fmaf_rn(fabsf(ah), 0x1p-19f, g);
@@ -163,14 +171,14 @@ __device__ __forceinline__ void step_f64(Chain<kPrec> &c, float h, double hp, fl
 #endif
 template <int kPrec, int kPx, int kPy, int kVar>
 constexpr int queue_min_blocks() {
-    return kPrec != TVS_PRECISION_MIXED64 ? 1
-           : kVar >= 3                    ? TVS_MIX_MIN_BLOCKS
+    return kVar >= 3                      ? TVS_MIX_MIN_BLOCKS
+           : kPrec != TVS_PRECISION_MIXED64 ? 1
            : kPx * kPy <= 2               ? TVS_MIX_MIN_BLOCKS
            : kPx * kPy == 4               ? 2
                                           : 1;
 }
 
-// MIXED64, one direction at a time.  A warp holds LX columns x 32/LX rows of
+// MIXED64 and exact f32, one direction at a time.  A warp holds LX columns x 32/LX rows of
 // lanes and each lane four points of view LX columns apart; the 8 warps of a
 // CTA stack in rows: a tile is 4 LX x 256/LX points (layout 1: LX = 8, 32 x 32;
 // layout 2: LX = 16, 64 x 16; layout 3: LX = 32, 128 x 8).  A lane sweeps its
@@ -184,18 +192,24 @@ __host__ __device__ constexpr int split_lx(int layout) { return 4 << layout; }
 __host__ __device__ constexpr int split_tile_w(int layout) { return kSplitCols * split_lx(layout); }
 __host__ __device__ constexpr int split_tile_h(int layout) { return kTileY * (32 / split_lx(layout)); }
 
-template <int LX, class Wait>
+// The filter threshold of an exact-f32 chain: m - |m| 2^-19 (one rounding).
+__device__ __forceinline__ float exact_lo(float m) { return __fmaf_rn(fabsf(m), -0x1p-19f, m); }
+
+template <int kPrec, int LX, class Wait>
 __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const QueueDem &D, uint32_t bx,
                                                  uint32_t by, uint32_t n, uint32_t n_fast,
                                                  const float4 *s_steps, const long long *s_boff,
-                                                 const double4 *s_dtab, double *s_fwd, Wait &&wait_prev) {
+                                                 const double4 *s_dtab, const float *s_zf,
+                                                 void *s_fwd_raw, Wait &&wait_prev) {
+    constexpr bool kMix = kPrec == TVS_PRECISION_MIXED64;
+    using S = typename std::conditional<kMix, double, float>::type;  // surfaces
     constexpr int K = kSplitCols, LY = 32 / LX;
     const uint32_t lx = threadIdx.x % LX, ly = threadIdx.x / LX;
     const uint32_t tx = bx * (K * LX) + lx;  // columns tx + LX k
     const uint32_t ty = D.row_begin + by * (kTileY * LY) + threadIdx.y * LY + ly;
     // rows past the grid are clamped, columns past it read padding; both are discarded
     const float *ep = D.elev + (int64_t)(min(ty, D.row_end - 1) + D.los) * D.width + tx + D.los;
-    float hp32[K];
+    float hp32[K];  // kernel.rs:134 (the exact-f32 observer elevation)
 #pragma unroll
     for (int k = 0; k < K; k++) hp32[k] = __fadd_rn(__ldg(ep + LX * k), D.observer_height);
     auto hp64 = [&](int k) -> double {
@@ -203,8 +217,9 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
     };
     // forward surfaces wait in shared memory (s_fwd[k * kThreads + tid]) while
     // the backward chains run
+    S *s_fwd = reinterpret_cast<S *>(s_fwd_raw);
     const uint32_t tid = threadIdx.y * kTileX + threadIdx.x;
-    double sb[K];
+    S sb[K];
     // one direction's sweep; DIR is a compile-time 0 (forward) or 1 (backward)
     auto pass = [&](auto DIR) {
         constexpr int dir = decltype(DIR)::value;
@@ -212,78 +227,129 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
             const long long b = s_boff[step];
             return (const float *)((const char *)ep + (dir ? -b : b));
         };
-        auto exact_angle = [&](int k, uint32_t step) -> double {
-            const double ek = __dsub_rn((double)__ldg(at(step) + LX * k), hp64(k));
-            const double4 dk = s_dtab[step];
-            return __dsub_rn(div_table64(ek, dk.x, dk.w), dk.y);
-        };
-        auto max64 = [&](int k, int32_t j) -> double {
-            return j < 0 ? -2000.0 : exact_angle(k, (uint32_t)j);
-        };
-        Chain<TVS_PRECISION_MIXED64> c[K];
-#pragma unroll
-        for (int k = 0; k < K; k++) c[k].init();
+        S out[K];
         uint32_t i = 0;
-        for (; i < n_fast; i++) {
-            const float4 t = s_steps[i];
-            const float *pe = at(i);
-            // filter (see the row layout): estimate + g >= m32 - gm
-            float e[K];
-            bool hit = false;
+        if constexpr (kMix) {
+            auto exact_angle = [&](int k, uint32_t step) -> double {
+                const double ek = __dsub_rn((double)__ldg(at(step) + LX * k), hp64(k));
+                const double4 dk = s_dtab[step];
+                return __dsub_rn(div_table64(ek, dk.x, dk.w), dk.y);
+            };
+            auto max64 = [&](int k, int32_t j) -> double {
+                return j < 0 ? -2000.0 : exact_angle(k, (uint32_t)j);
+            };
+            Chain<TVS_PRECISION_MIXED64> c[K];
 #pragma unroll
-            for (int k = 0; k < K; k++) {
-                e[k] = __fsub_rn(__ldg(pe + LX * k), hp32[k]);
-                hit |= __fmaf_rn(e[k], t.x, t.y) >= c[k].lo;
-            }
-            if (!__any_sync(0xffffffffu, hit)) continue;
-            const double w64 = s_dtab[i].z;
-            float ah[K], dd[K];
-            bool any_amb = false;
-#pragma unroll
-            for (int k = 0; k < K; k++) {
-                ah[k] = __fmaf_rn(e[k], t.x, t.z);
-                dd[k] = __fsub_rn(ah[k], c[k].m32);
-                const bool am = fabsf(dd[k]) <= __fadd_rn(t.w, c[k].gm);
-                if (!am && dd[k] > 0.0f) {  // surely visible
-                    c[k].set_max32(ah[k], t.w);
-                    c[k].j = (int32_t)i;
-                    c[k].s = __dadd_rn(c[k].s, w64);
-                }
-                any_amb |= am;
-            }
-            if (__any_sync(0xffffffffu, any_amb)) {
-                // a chain surely visible at this step has j == i; every other
-                // chain still has the state it was tested with
+            for (int k = 0; k < K; k++) c[k].init();
+            for (; i < n_fast; i++) {
+                const float4 t = s_steps[i];
+                const float *pe = at(i);
+                // filter (see the row layout): estimate + g >= m32 - gm
+                float e[K];
+                bool hit = false;
 #pragma unroll
                 for (int k = 0; k < K; k++) {
-                    if (c[k].j == (int32_t)i) continue;
-                    if (!(fabsf(dd[k]) <= __fadd_rn(t.w, c[k].gm))) continue;
-                    if (a.rechecks) atomicAdd(a.rechecks, 1ull);
-                    const double a64 = exact_angle(k, i);
-                    if (a64 > max64(k, c[k].j)) {
-                        c[k].j = (int32_t)i;
+                    e[k] = __fsub_rn(__ldg(pe + LX * k), hp32[k]);
+                    hit |= __fmaf_rn(e[k], t.x, t.y) >= c[k].lo;
+                }
+                if (!__any_sync(0xffffffffu, hit)) continue;
+                const double w64 = s_dtab[i].z;
+                float ah[K], dd[K];
+                bool any_amb = false;
+#pragma unroll
+                for (int k = 0; k < K; k++) {
+                    ah[k] = __fmaf_rn(e[k], t.x, t.z);
+                    dd[k] = __fsub_rn(ah[k], c[k].m32);
+                    const bool am = fabsf(dd[k]) <= __fadd_rn(t.w, c[k].gm);
+                    if (!am && dd[k] > 0.0f) {  // surely visible
                         c[k].set_max32(ah[k], t.w);
+                        c[k].j = (int32_t)i;
                         c[k].s = __dadd_rn(c[k].s, w64);
+                    }
+                    any_amb |= am;
+                }
+                if (__any_sync(0xffffffffu, any_amb)) {
+                    // a chain surely visible at this step has j == i; every other
+                    // chain still has the state it was tested with
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        if (c[k].j == (int32_t)i) continue;
+                        if (!(fabsf(dd[k]) <= __fadd_rn(t.w, c[k].gm))) continue;
+                        if (a.rechecks) atomicAdd(a.rechecks, 1ull);
+                        const double a64 = exact_angle(k, i);
+                        if (a64 > max64(k, c[k].j)) {
+                            c[k].j = (int32_t)i;
+                            c[k].set_max32(ah[k], t.w);
+                            c[k].s = __dadd_rn(c[k].s, w64);
+                        }
                     }
                 }
             }
-        }
 #pragma unroll
-        for (int k = 0; k < K; k++) c[k].m = max64(k, c[k].j);
-        // the steps past the table-division domain (zero distances), IEEE division
-        for (; i < n; i++) {
-            const double4 dt = s_dtab[i];
-            const float dist = (float)dt.w;
-            const int slow = !(dist >= 0x1p-20f && dist <= 0x1p20f);
-            const float *pe = at(i);
+            for (int k = 0; k < K; k++) c[k].m = max64(k, c[k].j);
+            // the steps past the table-division domain (zero distances), IEEE division
+            for (; i < n; i++) {
+                const double4 dt = s_dtab[i];
+                const float dist = (float)dt.w;
+                const int slow = !(dist >= 0x1p-20f && dist <= 0x1p20f);
+                const float *pe = at(i);
 #pragma unroll
-            for (int k = 0; k < K; k++)
-                step_f64<TVS_PRECISION_MIXED64, false>(c[k], __ldg(pe + LX * k), hp64(k), dist, dt, slow);
+                for (int k = 0; k < K; k++)
+                    step_f64<TVS_PRECISION_MIXED64, false>(c[k], __ldg(pe + LX * k), hp64(k), dist,
+                                                           dt, slow);
+            }
+#pragma unroll
+            for (int k = 0; k < K; k++) out[k] = c[k].s;
+        } else {
+            // Exact f32: the angle is computed exactly (kernel.rs:168-190) only at
+            // steps where some lane's estimate is not surely below its maximum:
+            // e y - d/R + g >= m - |m| 2^-19, where g >= 4 x 2^-22 (d/R + hmax/d)
+            // and |m| 2^-19 bound the estimate's distance from the exact angle
+            // with room for the test's own two roundings.  A skipped step has
+            // angle <= m (or NaN): not visible and no change of m, as in the
+            // reference.
+            Chain<TVS_PRECISION_EXACT32> c[K];
+            float lo[K];
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                c[k].init();
+                lo[k] = exact_lo(c[k].m);
+            }
+            for (; i < n_fast; i++) {
+                const float4 t = s_steps[i];
+                const float zf = s_zf[i];
+                const float *pe = at(i);
+                float e[K];
+                bool hit = false;
+#pragma unroll
+                for (int k = 0; k < K; k++) {
+                    e[k] = __fsub_rn(__ldg(pe + LX * k), hp32[k]);  // kernel.rs:164
+                    hit |= __fmaf_rn(e[k], t.x, zf) >= lo[k];
+                }
+                if (!__any_sync(0xffffffffu, hit)) continue;
+#pragma unroll
+                for (int k = 0; k < K; k++) {
+                    const float ang = __fsub_rn(div_table32(e[k], t.x, t.y), t.z);
+                    if (ang > c[k].m) c[k].s = __fadd_rn(c[k].s, t.w);
+                    c[k].m = fmaxf(ang, c[k].m);  // f32::max: NaN yields the other operand
+                    lo[k] = exact_lo(c[k].m);
+                }
+            }
+            for (; i < n; i++) {
+                const float4 t = s_steps[i];
+                const int slow = !(t.y >= 0x1p-20f && t.y <= 0x1p20f);
+                const float *pe = at(i);
+#pragma unroll
+                for (int k = 0; k < K; k++)
+                    step_f32<TVS_PRECISION_EXACT32, false>(c[k], __ldg(pe + LX * k), hp32[k], t, slow);
+            }
+#pragma unroll
+            for (int k = 0; k < K; k++) out[k] = c[k].s;
         }
 #pragma unroll
         for (int k = 0; k < K; k++) {
-            if (dir == 0) s_fwd[k * kThreads + tid] = c[k].s;
-            else sb[k] = c[k].s;
+            if (dir == 0) s_fwd[k * kThreads + tid] = out[k];
+            else sb[k] = out[k];
         }
     };
     pass(std::integral_constant<int, 0>{});
@@ -296,11 +362,19 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
         if (col >= D.tvs_width) continue;
         const uint64_t p = (uint64_t)ty * D.tvs_width + col;
         // forward surface first (kernel.rs:254), in L2 like the row layout
-        const double cum = __dadd_rn(__dadd_rn(__ldcg(D.cumulative64 + p), s_fwd[k * kThreads + tid]), sb[k]);
-        __stcg(D.cumulative64 + p, cum);
-        const float c32 = __double2float_rn(cum);
-        __stcg(D.cumulative + p, c32);
-        if (D.total) __stcg(D.total + p, __fadd_rn(__ldcg(D.total + p), c32));
+        if constexpr (kMix) {
+            const double cum =
+                __dadd_rn(__dadd_rn(__ldcg(D.cumulative64 + p), s_fwd[k * kThreads + tid]), sb[k]);
+            __stcg(D.cumulative64 + p, cum);
+            const float c32 = __double2float_rn(cum);
+            __stcg(D.cumulative + p, c32);
+            if (D.total) __stcg(D.total + p, __fadd_rn(__ldcg(D.total + p), c32));
+        } else {
+            const float cum =
+                __fadd_rn(__fadd_rn(__ldcg(D.cumulative + p), s_fwd[k * kThreads + tid]), sb[k]);
+            __stcg(D.cumulative + p, cum);
+            if (D.total) __stcg(D.total + p, __fadd_rn(__ldcg(D.total + p), cum));  // compute.rs:206-214
+        }
     }
 }
 
@@ -314,7 +388,7 @@ k_sweep_queue(QueueArgs a) {
     constexpr bool kPipe = kVar == 2;
     constexpr bool kSplit = kVar >= 3;
     constexpr bool kMix = kPrec == TVS_PRECISION_MIXED64;
-    static_assert(!kSplit || kMix, "the direction-split layout is MIXED64 only");
+    static_assert(!kSplit || kPrec != TVS_PRECISION_FP64, "no direction-split layout for FP64");
     constexpr bool kF64 = kPrec == TVS_PRECISION_FP64 || kMix;  // FP64 tables and surfaces
     extern __shared__ __align__(16) unsigned char smem[];
     QueueCtl &ctl = *reinterpret_cast<QueueCtl *>(smem);
@@ -360,7 +434,8 @@ k_sweep_queue(QueueArgs a) {
             const uint32_t n = h->n_steps;
             const float4 *gs = D.steps + (uint64_t)slot * D.step_cap;
             const int2 *go = D.offs + (uint64_t)slot * D.step_cap;
-            const float hmax = kMix ? *D.hmax : 0.0f;
+            const float hmax = (kMix || kSplit) ? *D.hmax : 0.0f;
+            float *s_zf = reinterpret_cast<float *>(s_boff + a.max_step_cap);  // exact f32 split only
             for (uint32_t i = tid; i < n; i += kThreads) {
                 const float4 t = gs[i];
                 s_steps[i] = t;
@@ -375,6 +450,11 @@ k_sweep_queue(QueueArgs a) {
                     s_steps[i] = make_float4(t.x, __fadd_rn(-t.z, g), -t.z, g);
                 }
                 s_boff[i] = (long long)go[i].x * (long long)sizeof(float);
+                if (kSplit && !kF64) {  // the exact-f32 filter's offset -d/R + g (g as above)
+                    const float g = __fadd_rn(__fmul_rn(0x1p-20f, __fadd_rn(t.z, __fmul_rn(hmax, t.x))),
+                                              0x1p-90f);
+                    s_zf[i] = __fadd_rn(-t.z, g);
+                }
                 if (kF64) {
                     double4 dv = D.dtab[(uint64_t)slot * D.step_cap + i];
                     if (kMix) dv.w = (double)t.y;
@@ -427,8 +507,10 @@ k_sweep_queue(QueueArgs a) {
         const uint32_t ty0 = D.row_begin + by * (kTileY * kPy) + threadIdx.y;
         if constexpr (kSplit) {
             if (run)
-                sweep_tile_split<split_lx(kVar - 2)>(a, D, bx, by, n, n_fast, s_steps, s_boff, s_dtab,
-                                 reinterpret_cast<double *>(s_dtab + a.max_step_cap), wait_prev);
+                sweep_tile_split<kPrec, split_lx(kVar - 2)>(
+                    a, D, bx, by, n, n_fast, s_steps, s_boff, s_dtab,
+                    reinterpret_cast<const float *>(s_boff + a.max_step_cap),
+                    reinterpret_cast<void *>(s_dtab + a.max_step_cap), wait_prev);
         } else if (run) {
             const float *ep[kPy];
             using HP = typename std::conditional<kF64, double, float>::type;
@@ -817,13 +899,20 @@ QueueConfig default_queue_config(int precision) {
         return d;
     }();
     // MIXED64 defaults to layout 2 (the fastest of the four on one B200 at
-    // 2401^2 and 3601^2); TVS_SWEEP_LAYOUT overrides it
+    // 2401^2 and 3601^2); TVS_SWEEP_LAYOUT overrides it, TVS_SWEEP_LAYOUT32
+    // the exact-f32 default (layout 0)
     static const int split = [] {
         const char *l = getenv("TVS_SWEEP_LAYOUT");
         return l ? atoi(l) : 2;
     }();
-    if (precision == TVS_PRECISION_MIXED64 && split >= 1 && split <= 3)
-        return QueueConfig{kSplitCols, 1, 0, 0, split};
+    static const int split32 = [] {
+        const char *l = getenv("TVS_SWEEP_LAYOUT32");
+        return l ? atoi(l) : 0;
+    }();
+    const int l = precision == TVS_PRECISION_MIXED64 ? split
+                  : precision == TVS_PRECISION_EXACT32 ? split32
+                                                       : 0;
+    if (l >= 1 && l <= 3) return QueueConfig{kSplitCols, 1, 0, 0, l};
     return v;
 }
 
@@ -852,11 +941,11 @@ cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, const QueueCon
     const bool f64 = precision == TVS_PRECISION_FP64;
     if (!f64 && !mix && precision != TVS_PRECISION_EXACT32) return cudaErrorInvalidValue;
     if (!queue_config_valid(c)) return cudaErrorInvalidValue;
-    if (c.layout != 0 && !mix) return cudaErrorInvalidValue;
+    if (c.layout != 0 && f64) return cudaErrorInvalidValue;
     const bool packed = c.packed && !f64 && !mix;
     const bool pipe = c.prefetch && !packed;
     // ctl + {steps, byte offsets} + FP64 double tables or packed exact-f32 tables (32 B each)
-    const bool wide = f64 || mix || packed;
+    const bool wide = f64 || mix || packed || c.layout != 0;
     // (+ the forward surfaces of the direction-split layout)
     const size_t smem = sizeof(QueueCtl) +
                         (size_t)a.max_step_cap * (sizeof(float4) + sizeof(long long) + (wide ? 32 : 0)) +
@@ -870,9 +959,12 @@ cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, const QueueCon
                : packed ? launch_queue_t<TVS_PRECISION_EXACT32, X, Y, 1>(a, smem, s)        \
                : pipe ? launch_queue_t<TVS_PRECISION_EXACT32, X, Y, 2>(a, smem, s)          \
                       : launch_queue_t<TVS_PRECISION_EXACT32, X, Y, 0>(a, smem, s);
-    if (c.layout == 1) return launch_queue_t<TVS_PRECISION_MIXED64, 1, 1, 3>(a, smem, s);
-    if (c.layout == 2) return launch_queue_t<TVS_PRECISION_MIXED64, 1, 1, 4>(a, smem, s);
-    if (c.layout == 3) return launch_queue_t<TVS_PRECISION_MIXED64, 1, 1, 5>(a, smem, s);
+#define TVS_L(L)                                                                  \
+    if (c.layout == L)                                                            \
+        return mix ? launch_queue_t<TVS_PRECISION_MIXED64, 1, 1, L + 2>(a, smem, s) \
+                   : launch_queue_t<TVS_PRECISION_EXACT32, 1, 1, L + 2>(a, smem, s);
+    TVS_L(1) TVS_L(2) TVS_L(3)
+#undef TVS_L
     TVS_Q(1, 1) TVS_Q(2, 1) TVS_Q(4, 1) TVS_Q(2, 2) TVS_Q(8, 1)
 #undef TVS_Q
     return cudaErrorInvalidValue;
