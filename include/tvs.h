@@ -153,6 +153,30 @@ int tvs_axes(tvs_context *ctx, uint32_t angle, uint64_t first_rank, uint64_t cou
 int tvs_band_shape(tvs_context *ctx, uint32_t angle, int32_t *band_deltas,
                    float *band_distances, uint32_t *band_steps_filled);
 
+/* A sector's band shape given as tables instead of computed, as when
+ * Compute::load_or_compute_cache (compute.rs:118-162) loads it from the cache
+ * (cache.rs:50-60).  Every later shape stage of that sector uses the first
+ * band_deltas_size entries of band_deltas/band_distances (n entries given):
+ * fewer than that -> TVS_ERR_SHAPE (the reference's kernel indexes past them);
+ * tables that fill more steps than this width and line of sight ->
+ * TVS_ERR_SHAPE.  tvs_band_shape then returns these tables.  Not used by
+ * batches or tvs_compute_sector_noalloc. */
+int tvs_set_band_shape(tvs_context *ctx, uint32_t angle, const int32_t *band_deltas,
+                       const float *band_distances, uint64_t n);
+/* Back to computed shapes for every sector. */
+int tvs_clear_band_shapes(tvs_context *ctx);
+/* The reference's shape cache (cache.rs:23-78) under state_directory (the
+ * reference uses the OS state directory, main.rs:63):
+ *   total-viewsheds/<width>/band_deltas/<angle>.bin   i32[band_deltas_size]
+ *   total-viewsheds/<width>/distances/<angle>.bin     f32[band_deltas_size]
+ * (raw, native-endian; a rectangular DEM uses <width>x<height>).  Load
+ * installs every sector whose two files exist (tvs_set_band_shape rules) and
+ * reports how many; save computes every sector's shape and writes its files,
+ * skipping sectors whose two files exist unless overwrite != 0 (the reference
+ * writes a sector's files when it had to compute them). */
+int tvs_cache_load(tvs_context *ctx, const char *state_directory, uint32_t *sectors_loaded);
+int tvs_cache_save(tvs_context *ctx, const char *state_directory, int overwrite);
+
 /* Compute::compute_sector (compute.rs:181-203) for ComputeType::Cuda:
  * cumulative_surfaces [computable_points_count] is read, advanced by this
  * sector and written back (kernel.rs:254).  FP64 and MIXED64 contexts widen

@@ -9,7 +9,7 @@
  * Every function restates one piece of tombh/total-viewsheds (Rust) and cites
  * the file:line it follows (paths relative to the reference repository).
  * Parity is pinned by the reference's own unit-test vectors (axes.rs:216-333,
- * band_of_sight.rs:230-315, cache.rs:443-461, compute.rs:306-416), transcribed
+ * band_of_sight.rs:230-315, cache.rs:87-105, compute.rs:306-416), transcribed
  * into tests/golden/reference_vectors.json by tests/golden/extract_reference_vectors.py.
  *
  * Rectangular DEMs (height != width) are an extension: the reference only

@@ -11,7 +11,7 @@ this file.  Run it where the reference checkout is present:
 Sources (paths inside the reference repository):
   crates/total-viewsheds/src/axes.rs:216-333         5x5 axes at 0 and 135 degrees
   crates/total-viewsheds/src/band_of_sight.rs:230-315  9x9 band shapes at 0/15/90/135
-  crates/total-viewsheds/src/cache.rs:443-461        9x9 shape at 35 degrees
+  crates/total-viewsheds/src/cache.rs:87-105        9x9 shape at 35 degrees
   crates/total-viewsheds/src/compute.rs:276-416      9x9 DEMs, totals, ASCII viewsheds
 """
 

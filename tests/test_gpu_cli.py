@@ -2,8 +2,10 @@
 a .bt DEM in (input.rs:86-175), `--compute cuda`, heatmap.png out
 (png.rs:5-37, compute.rs:165-178), checked against the oracle."""
 
+import os
 import struct
 import subprocess
+import tempfile
 import zlib
 
 import numpy as np
@@ -44,8 +46,14 @@ def expected_png(total):
     return v.astype(np.uint8)
 
 
-def run_cli(*args):
-    return subprocess.run([str(CLI), *map(str, args)], capture_output=True, text=True)
+# the CLI keeps the reference's shape cache in the OS state directory
+# ($XDG_STATE_HOME); the tests point it at a directory of their own
+STATE = tempfile.mkdtemp(prefix="tvs-state-")
+
+
+def run_cli(*args, state=STATE):
+    env = dict(os.environ, XDG_STATE_HOME=str(state))
+    return subprocess.run([str(CLI), *map(str, args)], capture_output=True, text=True, env=env)
 
 
 @pytest.fixture(scope="module")
@@ -98,3 +106,39 @@ def test_cli_rejects_other_backends_and_bad_input(bt, tmp_path):
     bt.write_bt(p, np.zeros((101, 101), np.float32))
     r = run_cli("--input", p, "--scale", 1, "--max-line-of-sight", 51)
     assert r.returncode == 1 and "longer than the maximum distance" in r.stderr
+
+
+def test_cli_shape_cache(bt, oracle, dem, tmp_path):
+    """compute.rs:118-162: the first run computes and saves every sector's shape
+    under <state>/total-viewsheds/<width>/, the second loads all 180 and gives
+    the same surfaces; another line of sight on the same width (the reference's
+    cache key is the width alone) is refused instead of misread; --no-cache
+    touches nothing."""
+    p = tmp_path / "dem.bt"
+    bt.write_bt(p, dem)
+    state = tmp_path / "state"
+    args = ("--input", p, "--scale", 30, "--observer-height", 1.65, "--heatmap", "final",
+            "--output-dir", tmp_path)
+    r1 = run_cli(*args, "--max-line-of-sight", 3000, "--surfaces-out", tmp_path / "a.bin",
+                 state=state)
+    assert r1.returncode == 0, r1.stderr
+    assert "0 of 180 sectors loaded" in r1.stderr
+    base = state / "total-viewsheds" / "301"
+    assert len(list((base / "band_deltas").glob("*.bin"))) == 180
+    assert len(list((base / "distances").glob("*.bin"))) == 180
+    g = oracle.geometry(301, 30.0, 3000)
+    d, x, _ = oracle.compile_band_data(g, 90.0)
+    assert np.array_equal(np.fromfile(base / "band_deltas" / "90.bin", np.int32), d)
+    assert np.array_equal(np.fromfile(base / "distances" / "90.bin", np.float32).view(np.uint32),
+                          x.view(np.uint32))
+    r2 = run_cli(*args, "--max-line-of-sight", 3000, "--surfaces-out", tmp_path / "b.bin",
+                 state=state)
+    assert r2.returncode == 0, r2.stderr
+    assert "180 of 180 sectors loaded" in r2.stderr
+    assert (tmp_path / "a.bin").read_bytes() == (tmp_path / "b.bin").read_bytes()
+    r3 = run_cli(*args, "--max-line-of-sight", 2400, state=state)
+    assert r3.returncode == 1 and "line of sight" in r3.stderr
+    fresh = tmp_path / "fresh"
+    r4 = run_cli(*args, "--max-line-of-sight", 3000, "--no-cache", state=fresh)
+    assert r4.returncode == 0, r4.stderr
+    assert not fresh.exists()

@@ -4,7 +4,7 @@ tests/golden/reference_vectors.json by extract_reference_vectors.py).
 Each test mirrors one reference test:
   axes.rs:216-333            at_0_degrees, at_135_degrees
   band_of_sight.rs:230-315   sector_at_{0,15,90,135}_degrees
-  cache.rs:443-461           saves_and_loads (shape at 35 degrees)
+  cache.rs:87-105           saves_and_loads (shape at 35 degrees)
   compute.rs:306-333         single_peak_totals, double_peak_totals
   compute.rs:358-416         viewsheds::{summit, off_summit, double_peak}
 Float vectors are compared bit for bit: Rust prints the shortest decimal that

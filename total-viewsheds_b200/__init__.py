@@ -118,6 +118,10 @@ SIGNATURES = {
     "tvs_set_elevations": (_INT, [_VP, _VP, _U64]),
     "tvs_axes": (_INT, [_VP, _U32, _U64, _U64, _VP, _VP]),
     "tvs_band_shape": (_INT, [_VP, _U32, _VP, _VP, _P(_U32)]),
+    "tvs_set_band_shape": (_INT, [_VP, _U32, _VP, _VP, _U64]),
+    "tvs_clear_band_shapes": (_INT, [_VP]),
+    "tvs_cache_load": (_INT, [_VP, ctypes.c_char_p, _P(_U32)]),
+    "tvs_cache_save": (_INT, [_VP, ctypes.c_char_p, _INT]),
     "tvs_compute_sector": (_INT, [_VP, _U32, _VP, _VP, _U64, _P(SectorStats)]),
     "tvs_run": (_INT, [_VP, _VP, _VP, _INT, SECTOR_CALLBACK, _VP]),
     "tvs_device_reset": (_INT, [_VP]),
@@ -267,6 +271,30 @@ class Engine:
         self._check(lib().tvs_band_shape(self.ctx, angle, _ptr(deltas), _ptr(dists),
                                          ctypes.byref(filled)))
         return deltas[:n], dists[:n], filled.value
+
+    def set_band_shape(self, angle, deltas, distances):
+        """Install a sector's band shape as tables (the reference's shape cache
+        entries, cache.rs:50-60) in place of the computed one."""
+        d = np.ascontiguousarray(deltas, np.int32)
+        x = np.ascontiguousarray(distances, np.float32)
+        self._check(lib().tvs_set_band_shape(self.ctx, angle, _ptr(d), _ptr(x),
+                                             min(d.size, x.size)))
+
+    def clear_band_shapes(self):
+        self._check(lib().tvs_clear_band_shapes(self.ctx))
+
+    def load_cache(self, state_directory):
+        """Install every sector found in the reference's shape cache under
+        state_directory (cache.rs:23-60); returns how many."""
+        n = ctypes.c_uint32()
+        self._check(lib().tvs_cache_load(self.ctx, os.fsencode(state_directory), ctypes.byref(n)))
+        return n.value
+
+    def save_cache(self, state_directory, overwrite=False):
+        """Write every sector's band shape in the reference's shape cache layout
+        (cache.rs:62-76); existing sector files are kept unless overwrite."""
+        self._check(lib().tvs_cache_save(self.ctx, os.fsencode(state_directory),
+                                         1 if overwrite else 0))
 
     def compute_sector(self, angle, cumulative, rings=None):
         """In place on cumulative (f32 [count]); rings (u32 [ring_slots]) receives the

@@ -136,7 +136,7 @@ void free_all(tvs_context *c) {
                     c->d_steps, c->d_offs, c->d_dtab, c->d_queue, c->d_done, c->d_error, c->d_hmax,
                     c->d_rechecks, c->d_qdem,
                     c->d_deltas, c->d_dists, c->d_rings, c->d_spill, c->d_counters, c->d_sf,
-                    c->d_sb};
+                    c->d_sb, c->d_tab_deltas, c->d_tab_dists, c->d_installed};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -265,6 +265,15 @@ int enqueue_shape(tvs_context *c, uint32_t first, uint32_t count) {
     tvs::ShapeArgs a = shape_args(c, first);
     TVS_CUDA(c, tvs::launch_shape(a, count, c->stream));
     c->launches++;
+    bool any = false;
+    for (uint32_t s = first; s < first + count && s < tvs::kSectorSteps; s++) any |= c->installed[s];
+    if (any) {  // installed tables replace the computed shapes of their sectors
+        const uint64_t bds = c->g.band_deltas_size;
+        TVS_CUDA(c, tvs::launch_shape_tables(a, count, c->d_tab_deltas + first * bds,
+                                             c->d_tab_dists + first * bds, c->d_installed + first,
+                                             c->stream));
+        c->launches++;
+    }
     for (uint32_t s = first; s < first + count && s < tvs::kSectorSteps; s++) c->pending[s] = true;
     return TVS_OK;
 }
@@ -466,6 +475,10 @@ tvs::QueueDem queue_dem_of(const tvs_context *c) { return queue_dem(c); }
 int header_status_of(tvs_context *c, uint32_t first, uint32_t count) {
     return header_status(c, first, count);
 }
+int fail_of(tvs_context *c, int code, const std::string &msg) { return fail(c, code, msg); }
+int enqueue_shape_of(tvs_context *c, uint32_t first, uint32_t count) {
+    return enqueue_shape(c, first, count);
+}
 }  // namespace tvs_host
 
 extern "C" {
@@ -621,9 +634,9 @@ int tvs_set_elevations(tvs_context *ctx, const float *elevations, uint64_t n) {
     TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
     TVS_CUDA(ctx, cudaMemcpyAsync(ctx->d_elev, elevations, n * sizeof(float),
                                   cudaMemcpyHostToDevice, ctx->stream));
-    if (ctx->p.precision == TVS_PRECISION_MIXED64)
-        TVS_CUDA(ctx, tvs::launch_max_abs(ctx->d_elev, n, ctx->p.observer_height, ctx->d_hmax,
-                                          ctx->stream));
+    // the estimate windows of the MIXED64 and filtered exact-f32 sweeps
+    TVS_CUDA(ctx, tvs::launch_max_abs(ctx->d_elev, n, ctx->p.observer_height, ctx->d_hmax,
+                                      ctx->stream));
     return TVS_OK;
 }
 

@@ -140,6 +140,77 @@ struct ShapeSmem {
 
 }  // namespace
 
+// Steps 5-7: the sweep's step tables from the prefix-summed forward offsets
+// soff[0, n_filled) and distances sdist[0, n_filled) in shared memory, the
+// path-bounds status and the header.  Steps past n_filled repeat the last
+// offset with d = 0.
+__device__ void finish_shape(const ShapeArgs &a, uint32_t sector, uint32_t n_filled,
+                             uint32_t n_steps, uint32_t n_cand, const long long *soff,
+                             const float *sdist, ShapeSmem &sm) {
+    ShapeHeader *hdr = a.hdr + sector;
+    long long mn = 0, mx = 0;
+    uint32_t first_slow = n_steps;
+    float4 *gsteps = a.steps + (uint64_t)sector * a.step_cap;
+    int2 *goffs = a.offs + (uint64_t)sector * a.step_cap;
+    for (uint32_t i = threadIdx.x; i < n_steps; i += blockDim.x) {
+        long long off = i < n_filled ? soff[i] : (n_filled ? soff[n_filled - 1] : 0);
+        float d = i < n_filled ? sdist[i] : 0.0f;
+        float4 st;
+        st.x = __frcp_rn(d);
+        st.y = d;
+        st.z = __fdiv_rn(d, kEarthRadiusSquared);
+        st.w = __fmul_rn(d, kTanOneRad);
+        int flags = (d >= 0x1p-20f && d <= 0x1p20f) ? 0 : kStepSlowDivide;
+        gsteps[i] = st;
+        goffs[i] = make_int2((int32_t)off, flags);
+        // FP64 sweep tables: the same distance in double (kernel.rs:175,216)
+        const double dd = (double)d;
+        a.dtab[(uint64_t)sector * a.step_cap + i] =
+            make_double4(__drcp_rn(dd), __ddiv_rn(dd, 12742000.0), __dmul_rn(dd, 0.0174533), 0.0);
+        mn = min(mn, off);
+        mx = max(mx, off);
+        if (flags) first_slow = min(first_slow, i);
+    }
+    __syncthreads();
+    sm.scan[threadIdx.x] = first_slow;
+    __syncthreads();
+    for (uint32_t o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sm.scan[threadIdx.x] = min(sm.scan[threadIdx.x], sm.scan[threadIdx.x + o]);
+        __syncthreads();
+    }
+    const uint32_t n_fast = (uint32_t)sm.scan[0];
+    __syncthreads();
+    // block min / max through the scan scratch
+    sm.scan[threadIdx.x] = mn;
+    __syncthreads();
+    for (uint32_t o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sm.scan[threadIdx.x] = min(sm.scan[threadIdx.x], sm.scan[threadIdx.x + o]);
+        __syncthreads();
+    }
+    const long long min_off = sm.scan[0];
+    __syncthreads();
+    sm.scan[threadIdx.x] = mx;
+    __syncthreads();
+    for (uint32_t o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sm.scan[threadIdx.x] = max(sm.scan[threadIdx.x], sm.scan[threadIdx.x + o]);
+        __syncthreads();
+    }
+    const long long max_off = sm.scan[0];
+    if (threadIdx.x == 0) {
+        // kernel.rs:157-164: every band of every point of view stays on the DEM.
+        const long long size = (long long)a.size;
+        bool ok = a.pov_min + min_off >= 0 && a.pov_max + max_off < size &&
+                  a.pov_min - max_off >= 0 && a.pov_max - min_off < size &&
+                  min_off >= INT32_MIN && max_off <= INT32_MAX;
+        hdr->status = ok ? TVS_OK : TVS_ERR_PATH_OUT_OF_DEM;
+        hdr->n_filled = n_filled;
+        hdr->n_steps = n_steps;
+        hdr->n_candidates = n_cand;
+        hdr->min_off = min_off;
+        hdr->max_off = max_off;
+        hdr->n_fast = n_fast;
+    }}
+
 // One sector of one DEM (the whole CTA).
 __device__ __forceinline__ void shape_sector(const ShapeArgs &a, const uint32_t sector,
                                              const uint64_t rank_lo, const uint64_t rank_count,
@@ -259,69 +330,7 @@ __device__ __forceinline__ void shape_sector(const ShapeArgs &a, const uint32_t 
     __syncthreads();
     block_inclusive_scan(soff, n_filled, sm.scan);
 
-    // 5. Step tables: steps past n_filled repeat the last offset with d = 0.
-    long long mn = 0, mx = 0;
-    uint32_t first_slow = n_steps;
-    float4 *gsteps = a.steps + (uint64_t)sector * a.step_cap;
-    int2 *goffs = a.offs + (uint64_t)sector * a.step_cap;
-    for (uint32_t i = threadIdx.x; i < n_steps; i += blockDim.x) {
-        long long off = i < n_filled ? soff[i] : (n_filled ? soff[n_filled - 1] : 0);
-        float d = i < n_filled ? sdist[i] : 0.0f;
-        float4 st;
-        st.x = __frcp_rn(d);
-        st.y = d;
-        st.z = __fdiv_rn(d, kEarthRadiusSquared);
-        st.w = __fmul_rn(d, kTanOneRad);
-        int flags = (d >= 0x1p-20f && d <= 0x1p20f) ? 0 : kStepSlowDivide;
-        gsteps[i] = st;
-        goffs[i] = make_int2((int32_t)off, flags);
-        // FP64 sweep tables: the same distance in double (kernel.rs:175,216)
-        const double dd = (double)d;
-        a.dtab[(uint64_t)sector * a.step_cap + i] =
-            make_double4(__drcp_rn(dd), __ddiv_rn(dd, 12742000.0), __dmul_rn(dd, 0.0174533), 0.0);
-        mn = min(mn, off);
-        mx = max(mx, off);
-        if (flags) first_slow = min(first_slow, i);
-    }
-    __syncthreads();
-    sm.scan[threadIdx.x] = first_slow;
-    __syncthreads();
-    for (uint32_t o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o) sm.scan[threadIdx.x] = min(sm.scan[threadIdx.x], sm.scan[threadIdx.x + o]);
-        __syncthreads();
-    }
-    const uint32_t n_fast = (uint32_t)sm.scan[0];
-    __syncthreads();
-    // block min / max through the scan scratch
-    sm.scan[threadIdx.x] = mn;
-    __syncthreads();
-    for (uint32_t o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o) sm.scan[threadIdx.x] = min(sm.scan[threadIdx.x], sm.scan[threadIdx.x + o]);
-        __syncthreads();
-    }
-    const long long min_off = sm.scan[0];
-    __syncthreads();
-    sm.scan[threadIdx.x] = mx;
-    __syncthreads();
-    for (uint32_t o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o) sm.scan[threadIdx.x] = max(sm.scan[threadIdx.x], sm.scan[threadIdx.x + o]);
-        __syncthreads();
-    }
-    const long long max_off = sm.scan[0];
-    if (threadIdx.x == 0) {
-        // kernel.rs:157-164: every band of every point of view stays on the DEM.
-        const long long size = (long long)a.size;
-        bool ok = a.pov_min + min_off >= 0 && a.pov_max + max_off < size &&
-                  a.pov_min - max_off >= 0 && a.pov_max - min_off < size &&
-                  min_off >= INT32_MIN && max_off <= INT32_MAX;
-        hdr->status = ok ? TVS_OK : TVS_ERR_PATH_OUT_OF_DEM;
-        hdr->n_filled = n_filled;
-        hdr->n_steps = n_steps;
-        hdr->n_candidates = n_cand;
-        hdr->min_off = min_off;
-        hdr->max_off = max_off;
-        hdr->n_fast = n_fast;
-    }
+    finish_shape(a, sector, n_filled, n_steps, n_cand, soff, sdist, sm);
 }
 
 __global__ void __launch_bounds__(kShapeThreads, 1)
@@ -335,6 +344,52 @@ k_shape_batch(const ShapeArgs *args, uint32_t n_sectors) {
     const ShapeArgs a = args[blockIdx.x / n_sectors];
     const uint64_t m = (uint64_t)a.win * a.win;
     shape_sector(a, blockIdx.x % n_sectors, m / 2 - a.band_samples / 2, a.band_samples, 0);
+}
+
+// A band shape given as tables instead of computed: the reference's shape
+// cache (cache.rs:50-60, read at compute.rs:132-140) holds the deltas and
+// distances of compile_band_data.  Sector b of the launch takes them from
+// tab_deltas/tab_dists + b * band_deltas_size when installed[b] != 0 and
+// overwrites the computed shape with them; its step tables follow as for a
+// computed shape.  The filled length is one past the last entry with a
+// nonzero delta or a distance other than +0 (the host has checked it against
+// the step-table capacity).
+__global__ void __launch_bounds__(kShapeThreads, 1)
+k_shape_tables(ShapeArgs a, const int32_t *tab_deltas, const float *tab_dists,
+               const unsigned char *installed) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ShapeSmem &sm = *reinterpret_cast<ShapeSmem *>(smem_raw);
+    const uint32_t sector = blockIdx.x;
+    if (!installed[sector]) return;
+    const uint32_t bds = a.band_deltas_size;
+    long long *soff = reinterpret_cast<long long *>(smem_raw + sizeof(ShapeSmem));
+    float *sdist = reinterpret_cast<float *>(soff + bds + 2);
+    const int32_t *td = tab_deltas + (uint64_t)sector * bds;
+    const float *tf = tab_dists + (uint64_t)sector * bds;
+    int32_t *gdel = a.deltas + (uint64_t)sector * bds;
+    float *gdist = a.dists + (uint64_t)sector * bds;
+    long long last = 0;
+    for (uint32_t i = threadIdx.x; i < bds; i += blockDim.x) {
+        const int32_t d = td[i];
+        const float x = tf[i];
+        gdel[i] = d;
+        gdist[i] = x;
+        soff[i] = d;
+        sdist[i] = x;
+        if (d != 0 || __float_as_uint(x) != 0u) last = (long long)i + 1;
+    }
+    __syncthreads();
+    sm.scan[threadIdx.x] = last;
+    __syncthreads();
+    for (uint32_t o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sm.scan[threadIdx.x] = max(sm.scan[threadIdx.x], sm.scan[threadIdx.x + o]);
+        __syncthreads();
+    }
+    const uint32_t n_filled = (uint32_t)sm.scan[0];
+    __syncthreads();
+    const uint32_t n_steps = n_filled + min(bds - n_filled, 2u);
+    block_inclusive_scan(soff, n_filled, sm.scan);
+    finish_shape(a, sector, n_filled, n_steps, 0, soff, sdist, sm);
 }
 
 // axes.rs:154-189: the f32 sight distance of every point.
@@ -355,6 +410,22 @@ cudaError_t launch_sight_distances(const SectorTrig &t, uint32_t width, uint32_t
 
 size_t shape_smem_bytes() {
     return sizeof(ShapeSmem) + (size_t)(kCandidateCap + kWindowCap) * sizeof(unsigned long long);
+}
+
+cudaError_t launch_shape_tables(const ShapeArgs &a, uint32_t n_sectors, const int32_t *tab_deltas,
+                                const float *tab_dists, const unsigned char *installed,
+                                cudaStream_t s) {
+    static bool configured = false;
+    const size_t smem = shape_smem_bytes();  // covers (bds + 2) * 8 + bds * 4 (host-checked)
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(k_shape_tables,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    if (n_sectors == 0) return cudaSuccess;
+    k_shape_tables<<<n_sectors, kShapeThreads, smem, s>>>(a, tab_deltas, tab_dists, installed);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_shape(const ShapeArgs &a, uint32_t n_sectors, cudaStream_t s) {

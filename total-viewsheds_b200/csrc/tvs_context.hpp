@@ -31,7 +31,7 @@ struct tvs_context {
     uint32_t *d_done = nullptr;
     uint32_t done_cap = 0;
     int32_t *d_error = nullptr;
-    float *d_hmax = nullptr;  // max |elevation| + |observer height| (MIXED64 window)
+    float *d_hmax = nullptr;  // max |elevation| + |observer height| (estimate windows)
     unsigned long long *d_rechecks = nullptr;  // MIXED64 FP64 re-decisions
     tvs::QueueDem *d_qdem = nullptr;           // this context as a one-DEM queue
     tvs::QueueConfig qcfg{0, 0, 0, 0, 0};            // sweep configuration (autotuned or default)
@@ -46,6 +46,12 @@ struct tvs_context {
     uint32_t spill_cap = 0;
     // plain-kernel scratch (allocated on first use)
     float *d_sf = nullptr, *d_sb = nullptr;
+    // band shapes installed as tables (the reference's shape cache), in place of
+    // computed ones; allocated on first use
+    int32_t *d_tab_deltas = nullptr;
+    float *d_tab_dists = nullptr;
+    unsigned char *d_installed = nullptr;  // [180]
+    bool installed[tvs::kSectorSteps] = {};
     // sectors whose shape stage ran since the last tvs_device_finish
     bool pending[tvs::kSectorSteps] = {};
     uint64_t device_bytes = 0;  // everything this context allocated on the device
@@ -57,4 +63,6 @@ namespace tvs_host {
 tvs::ShapeArgs shape_args_of(tvs_context *c, uint32_t first_slot);
 tvs::QueueDem queue_dem_of(const tvs_context *c);
 int header_status_of(tvs_context *c, uint32_t first, uint32_t count);
+int fail_of(tvs_context *c, int code, const std::string &msg);
+int enqueue_shape_of(tvs_context *c, uint32_t first, uint32_t count);
 }  // namespace tvs_host

@@ -180,6 +180,9 @@ __host__ __device__ inline uint32_t f32_radix_key(float f) {
 }
 
 // Host launchers (shape.cu, sweep.cu).
+cudaError_t launch_shape_tables(const ShapeArgs &a, uint32_t n_sectors, const int32_t *tab_deltas,
+                                const float *tab_dists, const unsigned char *installed,
+                                cudaStream_t s);
 cudaError_t launch_shape(const ShapeArgs &a, uint32_t n_sectors, cudaStream_t s);
 cudaError_t launch_sight_distances(const SectorTrig &t, uint32_t width, uint32_t height,
                                    float *out, cudaStream_t s);

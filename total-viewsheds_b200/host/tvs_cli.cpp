@@ -39,11 +39,22 @@ struct Options {
     std::string heatmap = "every-sector";
     std::string surfaces_out;
     int device = 0;
+    std::string state_directory;  // empty: the OS state directory (main.rs:63)
+    bool cache = true;
 };
 
 [[noreturn]] void die(const std::string &msg) {
     std::fprintf(stderr, "Error: %s\n", msg.c_str());
     std::exit(1);
+}
+
+// dirs::state_dir() on Linux: $XDG_STATE_HOME if absolute, else $HOME/.local/state.
+std::string os_state_directory() {
+    const char *x = std::getenv("XDG_STATE_HOME");
+    if (x && x[0] == '/') return x;
+    const char *h = std::getenv("HOME");
+    if (!h || !h[0]) die("Couldn't get the OS's state directory");
+    return std::string(h) + "/.local/state";
 }
 
 void usage() {
@@ -59,7 +70,9 @@ void usage() {
         "  --output-dir <DIR>             heatmap.png goes here [default: ./]\n"
         "  --scale <METRES>               override the DEM point spacing\n"
         "  --reference-observer-height    use the reference binary's hard-coded 1.8 m\n"
-        "  --precision <exact32|fp64>     sweep arithmetic [default: exact32]\n"
+        "  --precision <exact32|mixed64|fp64>  sweep arithmetic [default: exact32]\n"
+        "  --state-directory <DIR>        shape cache root [default: the OS state directory]\n"
+        "  --no-cache                     neither read nor write the shape cache\n"
         "  --heatmap <every-sector|final> heatmap.png cadence [default: every-sector]\n"
         "  --surfaces-out <PATH>          also write the f32 cumulative surfaces\n"
         "  --device <N>                   CUDA device [default: 0]\n");
@@ -86,6 +99,8 @@ Options parse(int argc, char **argv) {
         else if (a == "--heatmap") o.heatmap = val();
         else if (a == "--surfaces-out") o.surfaces_out = val();
         else if (a == "--device") o.device = std::atoi(val().c_str());
+        else if (a == "--state-directory") o.state_directory = val();
+        else if (a == "--no-cache") o.cache = false;
         else die("unknown argument " + a);
     }
     if (o.input.empty()) die("--input is required");
@@ -246,7 +261,9 @@ int main(int argc, char **argv) {
     p.max_line_of_sight = los;
     p.rings_per_km = o.rings_per_km;
     p.observer_height = o.reference_observer_height ? 1.8f : o.observer_height;
-    p.precision = o.precision == "fp64" ? TVS_PRECISION_FP64 : TVS_PRECISION_EXACT32;
+    p.precision = o.precision == "fp64"      ? TVS_PRECISION_FP64
+                  : o.precision == "mixed64" ? TVS_PRECISION_MIXED64
+                                             : TVS_PRECISION_EXACT32;
     p.sweep_kernel = TVS_SWEEP_ENGINE;
     p.device = o.device;
     std::fprintf(stderr, "Initialising: %ux%u DEM, scale %.3f m, line of sight %u m\n",
@@ -255,6 +272,14 @@ int main(int argc, char **argv) {
     check(tvs_create(&p, tile.heights.data(), (uint64_t)tile.width * tile.width, &ctx), nullptr);
     tvs_geometry g;
     tvs_get_geometry(ctx, &g);
+    if (o.cache) {  // compute.rs:118-162: load the cached shapes, compute and save the rest
+        const std::string dir = o.state_directory.empty() ? os_state_directory() : o.state_directory;
+        uint32_t loaded = 0;
+        check(tvs_cache_load(ctx, dir.c_str(), &loaded), ctx);
+        std::fprintf(stderr, "Shape cache %s/total-viewsheds/%u: %u of 180 sectors loaded\n",
+                     dir.c_str(), tile.width, loaded);
+        if (loaded < 180) check(tvs_cache_save(ctx, dir.c_str(), 0), ctx);
+    }
     std::vector<float> cumulative(g.computable_points_count), total(g.computable_points_count);
     const std::string heatmap = o.output_dir + "/heatmap.png";
     check(tvs_device_reset(ctx), ctx);
