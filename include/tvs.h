@@ -234,7 +234,8 @@ uint64_t tvs_device_bytes(const tvs_context *ctx);
  * time, evaluating angles exactly only where a warp's filter passes:
  * a warp holds LX = 4 << L columns x 32/LX rows of lanes, four points of view
  * per lane LX columns apart (tiles of 4 LX x 256/LX points); layout 2 is the
- * MIXED64 default.  Results do not depend on any of them. */
+ * MIXED64 default, layout 3 the EXACT32 one.  Results do not depend on any of
+ * them. */
 typedef struct tvs_sweep_config {
     int32_t points_x;
     int32_t points_y;

@@ -192,6 +192,13 @@ __host__ __device__ constexpr int split_lx(int layout) { return 4 << layout; }
 __host__ __device__ constexpr int split_tile_w(int layout) { return kSplitCols * split_lx(layout); }
 __host__ __device__ constexpr int split_tile_h(int layout) { return kTileY * (32 / split_lx(layout)); }
 
+// unroll factor of the direction-split fast loops (2: best of 1-4 on one B200)
+#ifndef TVS_SPLIT_UNROLL
+#define TVS_SPLIT_UNROLL 2
+#endif
+#define TVS_PRAGMA(x) _Pragma(#x)
+#define TVS_UNROLL(n) TVS_PRAGMA(unroll n)
+
 // The filter threshold of an exact-f32 chain: m - |m| 2^-19 (one rounding).
 __device__ __forceinline__ float exact_lo(float m) { return __fmaf_rn(fabsf(m), -0x1p-19f, m); }
 
@@ -241,6 +248,7 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
             Chain<TVS_PRECISION_MIXED64> c[K];
 #pragma unroll
             for (int k = 0; k < K; k++) c[k].init();
+            TVS_UNROLL(TVS_SPLIT_UNROLL)
             for (; i < n_fast; i++) {
                 const float4 t = s_steps[i];
                 const float *pe = at(i);
@@ -315,6 +323,7 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
                 c[k].init();
                 lo[k] = exact_lo(c[k].m);
             }
+            TVS_UNROLL(TVS_SPLIT_UNROLL)
             for (; i < n_fast; i++) {
                 const float4 t = s_steps[i];
                 const float zf = s_zf[i];
@@ -898,16 +907,16 @@ QueueConfig default_queue_config(int precision) {
         if (f) d.prefetch = atoi(f) != 0;
         return d;
     }();
-    // MIXED64 defaults to layout 2 (the fastest of the four on one B200 at
-    // 2401^2 and 3601^2); TVS_SWEEP_LAYOUT overrides it, TVS_SWEEP_LAYOUT32
-    // the exact-f32 default (layout 0)
+    // MIXED64 defaults to layout 2 and exact f32 to layout 3 (the fastest of
+    // the four on one B200 at 3601^2); TVS_SWEEP_LAYOUT and TVS_SWEEP_LAYOUT32
+    // override them
     static const int split = [] {
         const char *l = getenv("TVS_SWEEP_LAYOUT");
         return l ? atoi(l) : 2;
     }();
     static const int split32 = [] {
         const char *l = getenv("TVS_SWEEP_LAYOUT32");
-        return l ? atoi(l) : 0;
+        return l ? atoi(l) : 3;
     }();
     const int l = precision == TVS_PRECISION_MIXED64 ? split
                   : precision == TVS_PRECISION_EXACT32 ? split32
