@@ -164,9 +164,7 @@ __device__ void finish_shape(const ShapeArgs &a, uint32_t sector, uint32_t n_fil
         gsteps[i] = st;
         goffs[i] = make_int2((int32_t)off, flags);
         // FP64 sweep tables: the same distance in double (kernel.rs:175,216)
-        const double dd = (double)d;
-        a.dtab[(uint64_t)sector * a.step_cap + i] =
-            make_double4(__drcp_rn(dd), __ddiv_rn(dd, 12742000.0), __dmul_rn(dd, 0.0174533), 0.0);
+        a.dtab[(uint64_t)sector * a.step_cap + i] = fp64_step(d);
         mn = min(mn, off);
         mx = max(mx, off);
         if (flags) first_slow = min(first_slow, i);

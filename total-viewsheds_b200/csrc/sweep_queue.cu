@@ -102,6 +102,7 @@ struct QueueCtl {
     uint32_t n_steps;
     uint32_t n_fast;
     bool restage;
+    float hmax;             // the staged DEM's elevation range (estimate windows)
 };
 
 // Per-point state of one direction.
@@ -206,8 +207,9 @@ template <int kPrec, int LX, class Wait>
 __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const QueueDem &D, uint32_t bx,
                                                  uint32_t by, uint32_t n, uint32_t n_fast,
                                                  const float4 *s_steps, const long long *s_boff,
-                                                 const double4 *s_dtab, const float *s_zf,
-                                                 void *s_fwd_raw, Wait &&wait_prev) {
+                                                 const double *s_c64, const float *s_zf,
+                                                 const float &hmax, void *s_fwd_raw,
+                                                 Wait &&wait_prev) {
     constexpr bool kMix = kPrec == TVS_PRECISION_MIXED64;
     using S = typename std::conditional<kMix, double, float>::type;  // surfaces
     constexpr int K = kSplitCols, LY = 32 / LX;
@@ -238,9 +240,10 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
         uint32_t i = 0;
         if constexpr (kMix) {
             auto exact_angle = [&](int k, uint32_t step) -> double {
+                // the FP64 table values {1/d, d/R} of the shape stage (fp64_step)
                 const double ek = __dsub_rn((double)__ldg(at(step) + LX * k), hp64(k));
-                const double4 dk = s_dtab[step];
-                return __dsub_rn(div_table64(ek, dk.x, dk.w), dk.y);
+                const double dd = (double)s_steps[step].w;
+                return __dsub_rn(div_table64(ek, __drcp_rn(dd), dd), s_c64[step]);
             };
             auto max64 = [&](int k, int32_t j) -> double {
                 return j < 0 ? -2000.0 : exact_angle(k, (uint32_t)j);
@@ -261,16 +264,19 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
                     hit |= __fmaf_rn(e[k], t.x, t.y) >= c[k].lo;
                 }
                 if (!__any_sync(0xffffffffu, hit)) continue;
-                const double w64 = s_dtab[i].z;
+                const double w64 = __dmul_rn((double)t.w, 0.0174533);  // fp64_step(d).z
+                // the estimate window of the staging, recomputed bit for bit
+                const float gw = __fadd_rn(__fmul_rn(0x1p-20f, __fsub_rn(__fmul_rn(hmax, t.x), t.z)),
+                                           0x1p-90f);
                 float ah[K], dd[K];
                 bool any_amb = false;
 #pragma unroll
                 for (int k = 0; k < K; k++) {
                     ah[k] = __fmaf_rn(e[k], t.x, t.z);
                     dd[k] = __fsub_rn(ah[k], c[k].m32);
-                    const bool am = fabsf(dd[k]) <= __fadd_rn(t.w, c[k].gm);
+                    const bool am = fabsf(dd[k]) <= __fadd_rn(gw, c[k].gm);
                     if (!am && dd[k] > 0.0f) {  // surely visible
-                        c[k].set_max32(ah[k], t.w);
+                        c[k].set_max32(ah[k], gw);
                         c[k].j = (int32_t)i;
                         c[k].s = __dadd_rn(c[k].s, w64);
                     }
@@ -282,12 +288,12 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
 #pragma unroll
                     for (int k = 0; k < K; k++) {
                         if (c[k].j == (int32_t)i) continue;
-                        if (!(fabsf(dd[k]) <= __fadd_rn(t.w, c[k].gm))) continue;
+                        if (!(fabsf(dd[k]) <= __fadd_rn(gw, c[k].gm))) continue;
                         if (a.rechecks) atomicAdd(a.rechecks, 1ull);
                         const double a64 = exact_angle(k, i);
                         if (a64 > max64(k, c[k].j)) {
                             c[k].j = (int32_t)i;
-                            c[k].set_max32(ah[k], t.w);
+                            c[k].set_max32(ah[k], gw);
                             c[k].s = __dadd_rn(c[k].s, w64);
                         }
                     }
@@ -297,8 +303,9 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
             for (int k = 0; k < K; k++) c[k].m = max64(k, c[k].j);
             // the steps past the table-division domain (zero distances), IEEE division
             for (; i < n; i++) {
-                const double4 dt = s_dtab[i];
-                const float dist = (float)dt.w;
+                const float dist = s_steps[i].w;
+                const double dd = (double)dist;
+                const double4 dt = make_double4(__drcp_rn(dd), s_c64[i], __dmul_rn(dd, 0.0174533), dd);
                 const int slow = !(dist >= 0x1p-20f && dist <= 0x1p20f);
                 const float *pe = at(i);
 #pragma unroll
@@ -404,8 +411,13 @@ k_sweep_queue(QueueArgs a) {
     float4 *s_steps = reinterpret_cast<float4 *>(smem + sizeof(QueueCtl));
     // forward DEM-id offset of each step, in bytes (a 64-bit add per base address)
     long long *s_boff = reinterpret_cast<long long *>(s_steps + a.max_step_cap);
-    double4 *s_dtab = reinterpret_cast<double4 *>(s_boff + a.max_step_cap);  // FP64 only
+    double4 *s_dtab = reinterpret_cast<double4 *>(s_boff + a.max_step_cap);  // FP64 rows only
     PackedStep *s_pk = reinterpret_cast<PackedStep *>(s_boff + a.max_step_cap);  // packed only
+    // direction-split layouts: 8 B more per step (MIXED64: d/R in double;
+    // exact f32: the filter offset), then the forward surfaces
+    double *s_c64 = reinterpret_cast<double *>(s_boff + a.max_step_cap);
+    float *s_zf = reinterpret_cast<float *>(s_boff + a.max_step_cap);
+    void *s_fwd = s_c64 + a.max_step_cap;
     const uint32_t tid = threadIdx.y * kTileX + threadIdx.x;
     const uint32_t n_items = a.tiles_per_sector * a.n_sectors;
     if (tid == 0) {
@@ -444,30 +456,37 @@ k_sweep_queue(QueueArgs a) {
             const float4 *gs = D.steps + (uint64_t)slot * D.step_cap;
             const int2 *go = D.offs + (uint64_t)slot * D.step_cap;
             const float hmax = (kMix || kSplit) ? *D.hmax : 0.0f;
-            float *s_zf = reinterpret_cast<float *>(s_boff + a.max_step_cap);  // exact f32 split only
             for (uint32_t i = tid; i < n; i += kThreads) {
                 const float4 t = gs[i];
+                if constexpr (kSplit) {
+                    // the estimate window g as below
+                    const float g = __fadd_rn(__fmul_rn(0x1p-20f, __fadd_rn(t.z, __fmul_rn(hmax, t.x))),
+                                              0x1p-90f);
+                    s_boff[i] = (long long)go[i].x * (long long)sizeof(float);
+                    if constexpr (kMix) {
+                        // {1/d, filter offset, -d/R, d}: g is recomputed where needed
+                        s_steps[i] = make_float4(t.x, __fadd_rn(-t.z, g), -t.z, t.y);
+                        s_c64[i] = D.dtab[(uint64_t)slot * D.step_cap + i].y;
+                    } else {
+                        s_steps[i] = t;
+                        s_zf[i] = __fadd_rn(-t.z, g);
+                    }
+                    continue;
+                }
                 s_steps[i] = t;
                 if (kMix) {
                     // decision window of the FP32 estimate at this step: at least 4x
                     // the bound 2^-22 (|a| + d/R + hmax/d) on |estimate - FP64 angle|
                     // (the |a| part is carried with the running maximum).  The
-                    // filter's offset -d/R + g takes the place of d, which moves
-                    // to the FP64 table.
+                    // filter's offset -d/R + g takes the place of d, which the FP64
+                    // table also holds.
                     const float g = __fadd_rn(__fmul_rn(0x1p-20f, __fadd_rn(t.z, __fmul_rn(hmax, t.x))),
                                               0x1p-90f);
                     s_steps[i] = make_float4(t.x, __fadd_rn(-t.z, g), -t.z, g);
                 }
                 s_boff[i] = (long long)go[i].x * (long long)sizeof(float);
-                if (kSplit && !kF64) {  // the exact-f32 filter's offset -d/R + g (g as above)
-                    const float g = __fadd_rn(__fmul_rn(0x1p-20f, __fadd_rn(t.z, __fmul_rn(hmax, t.x))),
-                                              0x1p-90f);
-                    s_zf[i] = __fadd_rn(-t.z, g);
-                }
                 if (kF64) {
-                    double4 dv = D.dtab[(uint64_t)slot * D.step_cap + i];
-                    if (kMix) dv.w = (double)t.y;
-                    s_dtab[i] = dv;
+                    s_dtab[i] = D.dtab[(uint64_t)slot * D.step_cap + i];
                 } else if (kPacked) {  // only the packed loop reserves these 32 B per step
                     PackedStep p;
                     p.y = pk(t.x, t.x);
@@ -481,6 +500,7 @@ k_sweep_queue(QueueArgs a) {
                 ctl.sector_status = h->status;
                 ctl.n_steps = n;
                 ctl.n_fast = h->n_fast;
+                ctl.hmax = hmax;
             }
         }
         __syncthreads();  // the staged tables
@@ -517,9 +537,8 @@ k_sweep_queue(QueueArgs a) {
         if constexpr (kSplit) {
             if (run)
                 sweep_tile_split<kPrec, split_lx(kVar - 2)>(
-                    a, D, bx, by, n, n_fast, s_steps, s_boff, s_dtab,
-                    reinterpret_cast<const float *>(s_boff + a.max_step_cap),
-                    reinterpret_cast<void *>(s_dtab + a.max_step_cap), wait_prev);
+                    a, D, bx, by, n, n_fast, s_steps, s_boff, s_c64, s_zf, ctl.hmax, s_fwd,
+                    wait_prev);
         } else if (run) {
             const float *ep[kPy];
             using HP = typename std::conditional<kF64, double, float>::type;
@@ -953,12 +972,16 @@ cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, const QueueCon
     if (c.layout != 0 && f64) return cudaErrorInvalidValue;
     const bool packed = c.packed && !f64 && !mix;
     const bool pipe = c.prefetch && !packed;
-    // ctl + {steps, byte offsets} + FP64 double tables or packed exact-f32 tables (32 B each)
-    const bool wide = f64 || mix || packed || c.layout != 0;
-    // (+ the forward surfaces of the direction-split layout)
-    const size_t smem = sizeof(QueueCtl) +
-                        (size_t)a.max_step_cap * (sizeof(float4) + sizeof(long long) + (wide ? 32 : 0)) +
-                        (c.layout ? (size_t)kThreads * kSplitCols * sizeof(double) : 0);
+    // ctl + {steps, byte offsets} + FP64 double tables or packed exact-f32 tables
+    // (32 B each); the direction-split layouts instead take 8 B per step and the
+    // forward surfaces (8 B per point of view of the CTA)
+    const bool wide = f64 || mix || packed;
+    const size_t smem =
+        c.layout ? sizeof(QueueCtl) +
+                       (size_t)a.max_step_cap * (sizeof(float4) + 2 * sizeof(long long)) +
+                       (size_t)kThreads * kSplitCols * sizeof(double)
+                 : sizeof(QueueCtl) +
+                       (size_t)a.max_step_cap * (sizeof(float4) + sizeof(long long) + (wide ? 32 : 0));
 #define TVS_Q(X, Y)                                                                         \
     if (c.px == X && c.py == Y)                                                             \
         return mix ? (pipe ? launch_queue_t<TVS_PRECISION_MIXED64, X, Y, 2>(a, smem, s)      \

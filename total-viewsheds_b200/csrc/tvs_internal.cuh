@@ -21,6 +21,16 @@ namespace tvs {
 constexpr float kMaxAngle = -2000.0f;
 constexpr float kTanOneRad = 0.0174533f;
 constexpr float kEarthRadiusSquared = 12742000.0f;
+
+#ifdef __CUDACC__
+// The FP64 sweep's per-step values from the step's f32 distance d
+// (kernel.rs:175,216 in double): {1/d, d/R, d*tan1, d}.  The shape stage
+// tabulates them; sweeps short of shared memory recompute them from d.
+__device__ __forceinline__ double4 fp64_step(float d) {
+    const double dd = (double)d;
+    return make_double4(__drcp_rn(dd), __ddiv_rn(dd, 12742000.0), __dmul_rn(dd, 0.0174533), dd);
+}
+#endif
 constexpr float kSectorShift = 0.001f;
 constexpr uint32_t kSectorSteps = 180;
 
@@ -73,7 +83,7 @@ struct ShapeArgs {
     ShapeHeader *hdr;          // [sectors]
     float4 *steps;             // [sectors][step_cap]
     int2 *offs;                // [sectors][step_cap]
-    double4 *dtab;             // [sectors][step_cap] FP64 {1/d, d/R, d*tan1, 0}
+    double4 *dtab;             // [sectors][step_cap] FP64 {1/d, d/R, d*tan1, d}
     int32_t *deltas;           // [sectors][band_deltas_size]
     float *dists;              // [sectors][band_deltas_size]
     // Optional debug outputs for sector 0 of the launch (tvs_axes):
@@ -116,7 +126,7 @@ struct QueueDem {
     const ShapeHeader *hdr;            // per sector slot (absolute slot index)
     const float4 *steps;
     const int2 *offs;
-    const double4 *dtab;               // FP64 tables {1/d, d/R, d*tan1, 0} (double)
+    const double4 *dtab;               // FP64 tables {1/d, d/R, d*tan1, d} (double)
     float *cumulative;
     float *total;                      // nullable
     double *cumulative64;              // FP64/MIXED64 only
