@@ -97,7 +97,8 @@ class SweepConfig(ctypes.Structure):
 
     def __repr__(self):
         return (f"{self.points_x}x{self.points_y}{' packed' if self.packed else ''}"
-                f"{' prefetch' if self.prefetch else ''}{' split' if self.layout == 1 else ''}")
+                f"{' prefetch' if self.prefetch else ''}"
+                f"{f' split layout {self.layout}' if self.layout else ''}")
 
 
 SECTOR_CALLBACK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32,
