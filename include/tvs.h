@@ -230,12 +230,13 @@ uint64_t tvs_device_bytes(const tvs_context *ctx);
  * of 32*points_x x 8*points_y points; packed != 0 selects the packed f32x2
  * arithmetic (exact f32 only); prefetch != 0 issues the next step's elevation
  * loads before the current step's arithmetic (not with packed).  layout
- * L in 1..3 (MIXED64 and EXACT32, with points 4x1) sweeps one direction at a
- * time, evaluating angles exactly only where a warp's filter passes:
- * a warp holds LX = 4 << L columns x 32/LX rows of lanes, four points of view
- * per lane LX columns apart (tiles of 4 LX x 256/LX points); layout 2 is the
- * MIXED64 default, layout 3 the EXACT32 one.  Results do not depend on any of
- * them. */
+ * L in 1..6 (MIXED64 and EXACT32, with points 4x1) sweeps one direction at a
+ * time, evaluating angles exactly only where a warp's filter passes: a warp
+ * holds LX = 8, 16, 32 (L = 1, 2, 3 and again 4, 5, 6) columns x 32/LX rows of
+ * lanes; each lane has four points of view LX columns apart (L <= 3, tiles of
+ * 4 LX x 256/LX points) or 2 x 2 of them, LX columns and 32/LX rows apart
+ * (L >= 4, tiles of 2 LX x 512/LX).  Defaults: layout 2 for MIXED64, 6 for
+ * EXACT32, rows 2x1 for FP64.  Results do not depend on any of them. */
 typedef struct tvs_sweep_config {
     int32_t points_x;
     int32_t points_y;

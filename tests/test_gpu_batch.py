@@ -80,11 +80,12 @@ def test_sweep_configurations_agree(tvs, synth, shape):
 
 
 @pytest.mark.parametrize("w,h,rows", [(301, 301, None), (311, 197, None), (301, 301, (37, 90))])
-@pytest.mark.parametrize("layout", [0, 1, 2, 3])
+@pytest.mark.parametrize("layout", [0, 1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("precision,reference", [("mixed64", "fp64"), ("exact32", "exact32")])
 def test_split_layouts_agree(tvs, synth, w, h, layout, rows, precision, reference):
     """Every sweep layout (rows of lanes over both directions, and one direction
-    at a time over 8 x 4, 16 x 2 and 32 x 1 lanes) gives the reference sweep bit
+    at a time over 8 x 4, 16 x 2 and 32 x 1 lanes, with each lane's four points of
+    view in one row or in 2 x 2) gives the reference sweep bit
     for bit (MIXED64: the FP64 sweep; exact f32: the row layout, itself checked
     against the oracle elsewhere), on square and rectangular DEMs and on a row
     shard."""
@@ -135,7 +136,7 @@ def test_engine_autotune(tvs, synth):
 
 
 @pytest.mark.parametrize("kind", ["terraces", "steep"])
-@pytest.mark.parametrize("layout", [1, 2, 3])
+@pytest.mark.parametrize("layout", [1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("precision,reference", [("mixed64", "fp64"), ("exact32", "exact32")])
 def test_split_layouts_on_hard_terrain(tvs, synth, kind, layout, precision, reference):
     """The filtered layouts on terrain that stresses the filter: terraces (many

@@ -189,9 +189,16 @@ constexpr int queue_min_blocks() {
 // at fewer steps than when it mixes directions; narrower patches gain more
 // there and pay more L1 sectors per load (rows of LX * 4 bytes).
 constexpr int kSplitCols = 4;  // points of view per lane
-__host__ __device__ constexpr int split_lx(int layout) { return 4 << layout; }
-__host__ __device__ constexpr int split_tile_w(int layout) { return kSplitCols * split_lx(layout); }
-__host__ __device__ constexpr int split_tile_h(int layout) { return kTileY * (32 / split_lx(layout)); }
+// Layouts 4-6 are layouts 1-3 with each lane's four points of view as 2 columns
+// (LX apart) x 2 rows (32/LX apart): patches twice as tall and half as wide.
+__host__ __device__ constexpr int split_lx(int layout) { return 4 << ((layout - 1) % 3 + 1); }
+__host__ __device__ constexpr int split_ky(int layout) { return layout > 3 ? 2 : 1; }
+__host__ __device__ constexpr int split_tile_w(int layout) {
+    return kSplitCols / split_ky(layout) * split_lx(layout);
+}
+__host__ __device__ constexpr int split_tile_h(int layout) {
+    return kTileY * (32 / split_lx(layout)) * split_ky(layout);
+}
 
 // unroll factor of the direction-split fast loops (2: best of 1-4 on one B200)
 #ifndef TVS_SPLIT_UNROLL
@@ -203,7 +210,7 @@ __host__ __device__ constexpr int split_tile_h(int layout) { return kTileY * (32
 // The filter threshold of an exact-f32 chain: m - |m| 2^-19 (one rounding).
 __device__ __forceinline__ float exact_lo(float m) { return __fmaf_rn(fabsf(m), -0x1p-19f, m); }
 
-template <int kPrec, int LX, class Wait>
+template <int kPrec, int LX, int KY, class Wait>
 __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const QueueDem &D, uint32_t bx,
                                                  uint32_t by, uint32_t n, uint32_t n_fast,
                                                  const float4 *s_steps, const long long *s_boff,
@@ -212,17 +219,21 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
                                                  Wait &&wait_prev) {
     constexpr bool kMix = kPrec == TVS_PRECISION_MIXED64;
     using S = typename std::conditional<kMix, double, float>::type;  // surfaces
-    constexpr int K = kSplitCols, LY = 32 / LX;
+    constexpr int K = kSplitCols, KX = K / KY, LY = 32 / LX;
+    // chain k: column tx + LX (k % KX), row ty + LY (k / KX)
     const uint32_t lx = threadIdx.x % LX, ly = threadIdx.x / LX;
-    const uint32_t tx = bx * (K * LX) + lx;  // columns tx + LX k
-    const uint32_t ty = D.row_begin + by * (kTileY * LY) + threadIdx.y * LY + ly;
+    const uint32_t tx = bx * (KX * LX) + lx;
+    const uint32_t ty = D.row_begin + by * (kTileY * LY * KY) + threadIdx.y * LY * KY + ly;
     // rows past the grid are clamped, columns past it read padding; both are discarded
-    const float *ep = D.elev + (int64_t)(min(ty, D.row_end - 1) + D.los) * D.width + tx + D.los;
+    const float *ep[KY];
+#pragma unroll
+    for (int r = 0; r < KY; r++)
+        ep[r] = D.elev + (int64_t)(min(ty + LY * r, D.row_end - 1) + D.los) * D.width + tx + D.los;
     float hp32[K];  // kernel.rs:134 (the exact-f32 observer elevation)
 #pragma unroll
-    for (int k = 0; k < K; k++) hp32[k] = __fadd_rn(__ldg(ep + LX * k), D.observer_height);
+    for (int k = 0; k < K; k++) hp32[k] = __fadd_rn(__ldg(ep[k / KX] + LX * (k % KX)), D.observer_height);
     auto hp64 = [&](int k) -> double {
-        return __dadd_rn((double)__ldg(ep + LX * k), (double)D.observer_height);
+        return __dadd_rn((double)__ldg(ep[k / KX] + LX * (k % KX)), (double)D.observer_height);
     };
     // forward surfaces wait in shared memory (s_fwd[k * kThreads + tid]) while
     // the backward chains run
@@ -232,16 +243,17 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
     // one direction's sweep; DIR is a compile-time 0 (forward) or 1 (backward)
     auto pass = [&](auto DIR) {
         constexpr int dir = decltype(DIR)::value;
-        auto at = [&](uint32_t step) -> const float * {
+        // the sample of chain k at a step whose byte offset is b
+        auto at = [&](uint32_t step, int k) -> const float * {
             const long long b = s_boff[step];
-            return (const float *)((const char *)ep + (dir ? -b : b));
+            return (const float *)((const char *)ep[k / KX] + (dir ? -b : b)) + LX * (k % KX);
         };
         S out[K];
         uint32_t i = 0;
         if constexpr (kMix) {
             auto exact_angle = [&](int k, uint32_t step) -> double {
                 // the FP64 table values {1/d, d/R} of the shape stage (fp64_step)
-                const double ek = __dsub_rn((double)__ldg(at(step) + LX * k), hp64(k));
+                const double ek = __dsub_rn((double)__ldg(at(step, k)), hp64(k));
                 const double dd = (double)s_steps[step].w;
                 return __dsub_rn(div_table64(ek, __drcp_rn(dd), dd), s_c64[step]);
             };
@@ -254,13 +266,12 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
             TVS_UNROLL(TVS_SPLIT_UNROLL)
             for (; i < n_fast; i++) {
                 const float4 t = s_steps[i];
-                const float *pe = at(i);
                 // filter (see the row layout): estimate + g >= m32 - gm
                 float e[K];
                 bool hit = false;
 #pragma unroll
                 for (int k = 0; k < K; k++) {
-                    e[k] = __fsub_rn(__ldg(pe + LX * k), hp32[k]);
+                    e[k] = __fsub_rn(__ldg(at(i, k)), hp32[k]);
                     hit |= __fmaf_rn(e[k], t.x, t.y) >= c[k].lo;
                 }
                 if (!__any_sync(0xffffffffu, hit)) continue;
@@ -307,11 +318,10 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
                 const double dd = (double)dist;
                 const double4 dt = make_double4(__drcp_rn(dd), s_c64[i], __dmul_rn(dd, 0.0174533), dd);
                 const int slow = !(dist >= 0x1p-20f && dist <= 0x1p20f);
-                const float *pe = at(i);
 #pragma unroll
                 for (int k = 0; k < K; k++)
-                    step_f64<TVS_PRECISION_MIXED64, false>(c[k], __ldg(pe + LX * k), hp64(k), dist,
-                                                           dt, slow);
+                    step_f64<TVS_PRECISION_MIXED64, false>(c[k], __ldg(at(i, k)), hp64(k), dist, dt,
+                                                           slow);
             }
 #pragma unroll
             for (int k = 0; k < K; k++) out[k] = c[k].s;
@@ -334,12 +344,11 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
             for (; i < n_fast; i++) {
                 const float4 t = s_steps[i];
                 const float zf = s_zf[i];
-                const float *pe = at(i);
                 float e[K];
                 bool hit = false;
 #pragma unroll
                 for (int k = 0; k < K; k++) {
-                    e[k] = __fsub_rn(__ldg(pe + LX * k), hp32[k]);  // kernel.rs:164
+                    e[k] = __fsub_rn(__ldg(at(i, k)), hp32[k]);  // kernel.rs:164
                     hit |= __fmaf_rn(e[k], t.x, zf) >= lo[k];
                 }
                 if (!__any_sync(0xffffffffu, hit)) continue;
@@ -354,10 +363,9 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
             for (; i < n; i++) {
                 const float4 t = s_steps[i];
                 const int slow = !(t.y >= 0x1p-20f && t.y <= 0x1p20f);
-                const float *pe = at(i);
 #pragma unroll
                 for (int k = 0; k < K; k++)
-                    step_f32<TVS_PRECISION_EXACT32, false>(c[k], __ldg(pe + LX * k), hp32[k], t, slow);
+                    step_f32<TVS_PRECISION_EXACT32, false>(c[k], __ldg(at(i, k)), hp32[k], t, slow);
             }
 #pragma unroll
             for (int k = 0; k < K; k++) out[k] = c[k].s;
@@ -371,12 +379,12 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
     pass(std::integral_constant<int, 0>{});
     pass(std::integral_constant<int, 1>{});
     const bool write = wait_prev();  // every thread of the CTA reaches it
-    if (!write || ty >= D.row_end) return;
+    if (!write) return;
 #pragma unroll
     for (int k = 0; k < K; k++) {
-        const uint32_t col = tx + LX * k;
-        if (col >= D.tvs_width) continue;
-        const uint64_t p = (uint64_t)ty * D.tvs_width + col;
+        const uint32_t col = tx + LX * (k % KX), row = ty + LY * (k / KX);
+        if (col >= D.tvs_width || row >= D.row_end) continue;
+        const uint64_t p = (uint64_t)row * D.tvs_width + col;
         // forward surface first (kernel.rs:254), in L2 like the row layout
         if constexpr (kMix) {
             const double cum =
@@ -395,8 +403,8 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
 }
 
 // kVar: 0 scalar, 1 packed f32x2 (exact f32 only), 2 scalar with the next
-// step's elevations loaded while the current step computes, 3-5 the MIXED64
-// direction-split layouts 1-3 above (kPx, kPy unused).
+// step's elevations loaded while the current step computes, 3-8 the
+// direction-split layouts 1-6 above (kPx, kPy unused).
 template <int kPrec, int kPx, int kPy, int kVar>
 __global__ void __launch_bounds__(kThreads, (queue_min_blocks<kPrec, kPx, kPy, kVar>()))
 k_sweep_queue(QueueArgs a) {
@@ -536,7 +544,7 @@ k_sweep_queue(QueueArgs a) {
         const uint32_t ty0 = D.row_begin + by * (kTileY * kPy) + threadIdx.y;
         if constexpr (kSplit) {
             if (run)
-                sweep_tile_split<kPrec, split_lx(kVar - 2)>(
+                sweep_tile_split<kPrec, split_lx(kVar - 2), split_ky(kVar - 2)>(
                     a, D, bx, by, n, n_fast, s_steps, s_boff, s_c64, s_zf, ctl.hmax, s_fwd,
                     wait_prev);
         } else if (run) {
@@ -902,7 +910,7 @@ uint32_t queue_tiles_bound(uint32_t tvs_width, uint32_t rows) {
 }
 
 bool queue_config_valid(const QueueConfig &c) {
-    if (c.layout >= 1 && c.layout <= 3)
+    if (c.layout >= 1 && c.layout <= 6)
         return c.px == kSplitCols && c.py == 1 && !c.packed && !c.prefetch;
     if (c.layout != 0) return false;
     const int ok[][2] = {{1, 1}, {2, 1}, {4, 1}, {2, 2}, {8, 1}};
@@ -926,21 +934,20 @@ QueueConfig default_queue_config(int precision) {
         if (f) d.prefetch = atoi(f) != 0;
         return d;
     }();
-    // MIXED64 defaults to layout 2 and exact f32 to layout 3 (the fastest of
-    // the four on one B200 at 3601^2); TVS_SWEEP_LAYOUT and TVS_SWEEP_LAYOUT32
-    // override them
+    // MIXED64 defaults to layout 2 and exact f32 to layout 6 (the fastest on
+    // one B200 at 3601^2); TVS_SWEEP_LAYOUT and TVS_SWEEP_LAYOUT32 override them
     static const int split = [] {
         const char *l = getenv("TVS_SWEEP_LAYOUT");
         return l ? atoi(l) : 2;
     }();
     static const int split32 = [] {
         const char *l = getenv("TVS_SWEEP_LAYOUT32");
-        return l ? atoi(l) : 3;
+        return l ? atoi(l) : 6;
     }();
     const int l = precision == TVS_PRECISION_MIXED64 ? split
                   : precision == TVS_PRECISION_EXACT32 ? split32
                                                        : 0;
-    if (l >= 1 && l <= 3) return QueueConfig{kSplitCols, 1, 0, 0, l};
+    if (l >= 1 && l <= 6) return QueueConfig{kSplitCols, 1, 0, 0, l};
     return v;
 }
 
@@ -995,7 +1002,7 @@ cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, const QueueCon
     if (c.layout == L)                                                            \
         return mix ? launch_queue_t<TVS_PRECISION_MIXED64, 1, 1, L + 2>(a, smem, s) \
                    : launch_queue_t<TVS_PRECISION_EXACT32, 1, 1, L + 2>(a, smem, s);
-    TVS_L(1) TVS_L(2) TVS_L(3)
+    TVS_L(1) TVS_L(2) TVS_L(3) TVS_L(4) TVS_L(5) TVS_L(6)
 #undef TVS_L
     TVS_Q(1, 1) TVS_Q(2, 1) TVS_Q(4, 1) TVS_Q(2, 2) TVS_Q(8, 1)
 #undef TVS_Q
