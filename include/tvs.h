@@ -187,6 +187,19 @@ int tvs_cache_save(tvs_context *ctx, const char *state_directory, int overwrite)
 int tvs_compute_sector(tvs_context *ctx, uint32_t angle, float *cumulative_surfaces,
                        uint32_t *rings, uint64_t rings_len, tvs_sector_stats *stats);
 
+/* The sector's ring records as a compact stream instead of the reference's
+ * reserved slots (kernel.rs:141-145,220-243,302-309, 2.08 GB per sector at
+ * 3601^2 with mostly empty slots): band k's record (pov, closing, opening,
+ * closing, ... -- the n ids after the reference's count slot, never truncated
+ * by the reservation) is ids[band_offsets[k] .. band_offsets[k+1]).  This call
+ * advances cumulative_surfaces as tvs_compute_sector does, keeps the records
+ * on the device and returns their id count; tvs_read_ring_records copies
+ * band_offsets [total_bands + 1] (u64) and ids [*total_ids] (either nullable).
+ * No counterpart in the reference; the records equal its per-band records. */
+int tvs_compute_sector_rings(tvs_context *ctx, uint32_t angle, float *cumulative_surfaces,
+                             uint64_t *total_ids, tvs_sector_stats *stats);
+int tvs_read_ring_records(tvs_context *ctx, uint64_t *band_offsets, uint32_t *ids);
+
 /* Compute::run (compute.rs:101-115): all 180 sectors.  cumulative_out and
  * total_out (the heatmap running total, compute.rs:206-214; nullable) have
  * computable_points_count entries.  callback (nullable) receives each

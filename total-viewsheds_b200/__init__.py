@@ -120,6 +120,8 @@ SIGNATURES = {
     "tvs_axes": (_INT, [_VP, _U32, _U64, _U64, _VP, _VP]),
     "tvs_band_shape": (_INT, [_VP, _U32, _VP, _VP, _P(_U32)]),
     "tvs_set_band_shape": (_INT, [_VP, _U32, _VP, _VP, _U64]),
+    "tvs_compute_sector_rings": (_INT, [_VP, _U32, _VP, _P(_U64), _P(SectorStats)]),
+    "tvs_read_ring_records": (_INT, [_VP, _VP, _VP]),
     "tvs_clear_band_shapes": (_INT, [_VP]),
     "tvs_cache_load": (_INT, [_VP, ctypes.c_char_p, _P(_U32)]),
     "tvs_cache_save": (_INT, [_VP, ctypes.c_char_p, _INT]),
@@ -272,6 +274,20 @@ class Engine:
         self._check(lib().tvs_band_shape(self.ctx, angle, _ptr(deltas), _ptr(dists),
                                          ctypes.byref(filled)))
         return deltas[:n], dists[:n], filled.value
+
+    def compute_sector_rings(self, angle, cumulative):
+        """One sector, in place on cumulative, with its ring records as a compact
+        stream: (band_offsets u64 [total_bands + 1], ids u32, SectorStats); band
+        k's record is ids[band_offsets[k]:band_offsets[k + 1]]."""
+        assert cumulative.dtype == np.float32 and cumulative.flags.c_contiguous
+        total = ctypes.c_uint64()
+        st = SectorStats()
+        self._check(lib().tvs_compute_sector_rings(self.ctx, angle, _ptr(cumulative),
+                                                   ctypes.byref(total), ctypes.byref(st)))
+        offsets = np.empty(self.geometry.total_bands + 1, np.uint64)
+        ids = np.empty(max(total.value, 1), np.uint32)
+        self._check(lib().tvs_read_ring_records(self.ctx, _ptr(offsets), _ptr(ids)))
+        return offsets, ids[:total.value], st
 
     def set_band_shape(self, angle, deltas, distances):
         """Install a sector's band shape as tables (the reference's shape cache

@@ -136,7 +136,8 @@ void free_all(tvs_context *c) {
                     c->d_steps, c->d_offs, c->d_dtab, c->d_queue, c->d_done, c->d_error, c->d_hmax,
                     c->d_rechecks, c->d_qdem,
                     c->d_deltas, c->d_dists, c->d_rings, c->d_spill, c->d_counters, c->d_sf,
-                    c->d_sb, c->d_tab_deltas, c->d_tab_dists, c->d_installed};
+                    c->d_sb, c->d_tab_deltas, c->d_tab_dists, c->d_installed,
+                    c->d_rc_blocks, c->d_rc_offsets, c->d_rc_ids};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -754,6 +755,98 @@ int tvs_compute_sector(tvs_context *ctx, uint32_t angle, float *cumulative_surfa
         rc = collect_rings(ctx, rings, rings_len, stats);
         if (rc) return rc;
     }
+    TVS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return TVS_OK;
+}
+
+int tvs_compute_sector_rings(tvs_context *ctx, uint32_t angle, float *cumulative_surfaces,
+                             uint64_t *total_ids, tvs_sector_stats *stats) {
+    if (!ctx || !cumulative_surfaces || !total_ids) return TVS_ERR_INVALID_ARGUMENT;
+    if (angle >= tvs::kSectorSteps) return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "angle >= 180");
+    TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
+    ctx->rc_valid = false;
+    const uint64_t count = ctx->g.computable_points_count;
+    if (count)
+        TVS_CUDA(ctx, cudaMemcpyAsync(ctx->d_cum, cumulative_surfaces, count * sizeof(float),
+                                      cudaMemcpyHostToDevice, ctx->stream));
+    if (ctx->d_cum64 && count)
+        TVS_CUDA(ctx, tvs::launch_widen(ctx->d_cum, ctx->d_cum64, count, ctx->stream));
+    int rc = ensure_rings(ctx);
+    if (rc) return rc;
+    const uint64_t bands = ctx->g.total_bands;
+    const uint32_t R = ctx->g.reserved_rings_per_band;
+    const uint64_t nb = tvs::ring_scan_blocks(bands);
+    if (!ctx->d_rc_offsets) {
+        TVS_CUDA(ctx, cudaMalloc(&ctx->d_rc_offsets, (bands + 1) * sizeof(uint64_t)));
+        TVS_CUDA(ctx, cudaMalloc(&ctx->d_rc_blocks, (nb + 1) * sizeof(uint64_t)));
+        ctx->device_bytes += (bands + 1 + nb + 1) * sizeof(uint64_t);
+    }
+    TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_rings, 0, ctx->g.ring_slots_per_sector * sizeof(uint32_t),
+                                  ctx->stream));
+    TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), ctx->stream));
+    rc = enqueue_shape(ctx, angle, 1);
+    if (rc) return rc;
+    rc = header_status(ctx, angle, 1);
+    if (rc) return rc;
+    rc = enqueue_sweep(ctx, angle, 1, true);
+    if (rc) return rc;
+    if (count)
+        TVS_CUDA(ctx, cudaMemcpyAsync(cumulative_surfaces, ctx->d_cum, count * sizeof(float),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+    uint32_t cnt[4];
+    TVS_CUDA(ctx, cudaMemcpyAsync(cnt, ctx->d_counters, sizeof cnt, cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    TVS_CUDA(ctx, tvs::launch_ring_count(ctx->d_rings, bands, R, ctx->d_rc_blocks, ctx->stream));
+    uint64_t total = 0;
+    TVS_CUDA(ctx, cudaMemcpyAsync(&total, ctx->d_rc_blocks + nb, sizeof total,
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    TVS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (stats) {
+        std::memset(stats, 0, sizeof *stats);
+        stats->angle = angle;
+        stats->band_steps_filled = ctx->g.band_steps_filled;
+        stats->overflow_bands = cnt[1];
+        stats->max_ring_ids = cnt[2];
+        stats->spill_entries = cnt[0];
+    }
+    if (cnt[0] > ctx->spill_cap)
+        return fail(ctx, TVS_ERR_CAPACITY, "ring spill list capacity exceeded");
+    if (total > ctx->rc_ids_cap) {
+        if (ctx->d_rc_ids) {
+            cudaFree(ctx->d_rc_ids);
+            ctx->device_bytes -= ctx->rc_ids_cap * sizeof(uint32_t);
+            ctx->d_rc_ids = nullptr;
+            ctx->rc_ids_cap = 0;
+        }
+        const uint64_t cap = total + total / 4;  // room for the next sectors
+        TVS_CUDA(ctx, cudaMalloc(&ctx->d_rc_ids, std::max<uint64_t>(cap, 1) * sizeof(uint32_t)));
+        ctx->rc_ids_cap = std::max<uint64_t>(cap, 1);
+        ctx->device_bytes += ctx->rc_ids_cap * sizeof(uint32_t);
+    }
+    if (bands == 0)
+        TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_rc_offsets, 0, sizeof(uint64_t), ctx->stream));
+    TVS_CUDA(ctx, tvs::launch_ring_gather(ctx->d_rings, bands, R, ctx->d_rc_blocks, ctx->d_spill,
+                                          cnt[0], ctx->d_rc_offsets, ctx->d_rc_ids, ctx->stream));
+    ctx->launches += 2;
+    TVS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->rc_total = total;
+    ctx->rc_valid = true;
+    *total_ids = total;
+    return TVS_OK;
+}
+
+int tvs_read_ring_records(tvs_context *ctx, uint64_t *band_offsets, uint32_t *ids) {
+    if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
+    if (!ctx->rc_valid)
+        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "no ring records: call tvs_compute_sector_rings");
+    TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
+    if (band_offsets)
+        TVS_CUDA(ctx, cudaMemcpyAsync(band_offsets, ctx->d_rc_offsets,
+                                      (ctx->g.total_bands + 1) * sizeof(uint64_t),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+    if (ids && ctx->rc_total)
+        TVS_CUDA(ctx, cudaMemcpyAsync(ids, ctx->d_rc_ids, ctx->rc_total * sizeof(uint32_t),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
     TVS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return TVS_OK;
 }

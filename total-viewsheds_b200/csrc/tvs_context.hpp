@@ -52,6 +52,12 @@ struct tvs_context {
     float *d_tab_dists = nullptr;
     unsigned char *d_installed = nullptr;  // [180]
     bool installed[tvs::kSectorSteps] = {};
+    // compact ring records of the last tvs_compute_sector_rings (allocated on first use)
+    uint64_t *d_rc_blocks = nullptr;   // scanned record-length block sums
+    uint64_t *d_rc_offsets = nullptr;  // [total_bands + 1]
+    uint32_t *d_rc_ids = nullptr;
+    uint64_t rc_ids_cap = 0, rc_total = 0;
+    bool rc_valid = false;
     // sectors whose shape stage ran since the last tvs_device_finish
     bool pending[tvs::kSectorSteps] = {};
     uint64_t device_bytes = 0;  // everything this context allocated on the device

@@ -190,6 +190,15 @@ __host__ __device__ inline uint32_t f32_radix_key(float f) {
 }
 
 // Host launchers (shape.cu, sweep.cu).
+// Compact ring records (rings_compact.cu): block sums of the record lengths
+// (ring_scan_blocks(bands) + 1 entries, exclusive-scanned, total last), then
+// the offsets and ids.
+uint64_t ring_scan_blocks(uint64_t bands);
+cudaError_t launch_ring_count(const uint32_t *rings, uint64_t bands, uint32_t reserved,
+                              uint64_t *block_sums, cudaStream_t s);
+cudaError_t launch_ring_gather(const uint32_t *rings, uint64_t bands, uint32_t reserved,
+                               const uint64_t *block_sums, const uint4 *spill, uint32_t n_spill,
+                               uint64_t *offsets, uint32_t *ids, cudaStream_t s);
 cudaError_t launch_shape_tables(const ShapeArgs &a, uint32_t n_sectors, const int32_t *tab_deltas,
                                 const float *tab_dists, const unsigned char *installed,
                                 cudaStream_t s);
