@@ -137,7 +137,7 @@ void free_all(tvs_context *c) {
                     c->d_rechecks, c->d_qdem,
                     c->d_deltas, c->d_dists, c->d_rings, c->d_spill, c->d_counters, c->d_sf,
                     c->d_sb, c->d_tab_deltas, c->d_tab_dists, c->d_installed,
-                    c->d_rc_blocks, c->d_rc_offsets, c->d_rc_ids};
+                    c->d_rc_blocks, c->d_rc_offsets, c->d_rc_ids, c->d_bmax};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -299,6 +299,9 @@ tvs::QueueDem queue_dem(const tvs_context *c) {
     d.total = c->d_total;
     d.cumulative64 = c->d_cum64;
     d.hmax = c->d_hmax;
+    d.bmax = c->d_bmax;
+    d.bmax_w = c->bmax_w;
+    d.bmax_h = c->bmax_h;
     return d;
 }
 
@@ -535,6 +538,8 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
     }
     c->step_cap = (g.band_steps_filled + 2 + 3) & ~3u;
     c->done_cap = tvs::queue_tiles_bound(g.tvs_width, re - rb);
+    c->bmax_w = (g.width + tvs::kBlockMax - 1) / tvs::kBlockMax;
+    c->bmax_h = (g.height + tvs::kBlockMax - 1) / tvs::kBlockMax;
     c->qcfg = tvs::default_queue_config((int)c->p.precision);
     auto bail = [&](cudaError_t e, const char *what) {
         std::string m = std::string(what) + ": " + cudaGetErrorString(e);
@@ -564,6 +569,7 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
         {(void **)&c->d_done, (size_t)std::max<uint32_t>(c->done_cap, 1) * sizeof(uint32_t)},
         {(void **)&c->d_error, sizeof(int32_t)},
         {(void **)&c->d_hmax, sizeof(float)},
+        {(void **)&c->d_bmax, (size_t)std::max<uint64_t>((uint64_t)c->bmax_w * c->bmax_h, 1) * sizeof(float)},
         {(void **)&c->d_rechecks, sizeof(unsigned long long)},
         {(void **)&c->d_qdem, sizeof(tvs::QueueDem)},
         {(void **)&c->d_deltas, (size_t)slots * bds * sizeof(int32_t)},
@@ -600,6 +606,7 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
         return bail(e, "cudaMemset elevation padding");
     if ((e = tvs::launch_max_abs(c->d_elev, g.size, params->observer_height, c->d_hmax, 0)) !=
             cudaSuccess ||
+        (e = tvs::launch_block_max(c->d_elev, g.width, g.height, c->d_bmax, 0)) != cudaSuccess ||
         (e = cudaDeviceSynchronize()) != cudaSuccess)
         return bail(e, "elevation range");
     if ((e = cudaMemset(c->d_hdr, 0, slots * sizeof(tvs::ShapeHeader))) != cudaSuccess ||
@@ -638,6 +645,8 @@ int tvs_set_elevations(tvs_context *ctx, const float *elevations, uint64_t n) {
     // the estimate windows of the MIXED64 and filtered exact-f32 sweeps
     TVS_CUDA(ctx, tvs::launch_max_abs(ctx->d_elev, n, ctx->p.observer_height, ctx->d_hmax,
                                       ctx->stream));
+    TVS_CUDA(ctx, tvs::launch_block_max(ctx->d_elev, ctx->g.width, ctx->g.height, ctx->d_bmax,
+                                        ctx->stream));
     return TVS_OK;
 }
 

@@ -471,12 +471,32 @@ __global__ void k_max_abs(const float *x, uint64_t n, float add, unsigned int *o
     if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(__fadd_ru(m, fabsf(add))));
 }
 
+__global__ void k_block_max(const float *elev, uint32_t W, uint32_t H, float *bmax) {
+    const uint32_t bw = (W + kBlockMax - 1) / kBlockMax, bh = (H + kBlockMax - 1) / kBlockMax;
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= bw * bh) return;
+    const uint32_t bx = b % bw, by = b / bw;
+    float m = -INFINITY;
+    for (uint32_t y = by * kBlockMax; y < min(H, (by + 1) * kBlockMax); y++)
+        for (uint32_t x = bx * kBlockMax; x < min(W, (bx + 1) * kBlockMax); x++)
+            m = fmaxf(m, elev[(uint64_t)y * W + x]);
+    bmax[b] = m;
+}
+
 __global__ void k_widen(const float *x, double *y, uint64_t n) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) y[i] = (double)x[i];
 }
 
 }  // namespace
+
+cudaError_t launch_block_max(const float *elev, uint32_t W, uint32_t H, float *bmax,
+                             cudaStream_t s) {
+    const uint32_t n = ((W + kBlockMax - 1) / kBlockMax) * ((H + kBlockMax - 1) / kBlockMax);
+    if (n == 0) return cudaSuccess;
+    k_block_max<<<(n + 255) / 256, 256, 0, s>>>(elev, W, H, bmax);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_widen(const float *x, double *y, uint64_t n, cudaStream_t s) {
     if (n == 0) return cudaSuccess;

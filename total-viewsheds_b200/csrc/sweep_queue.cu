@@ -26,6 +26,7 @@
 // TVS_PRECISION_FP64 (the same control flow in double: angles, maximum and
 // surfaces; table division in double from y = RN64(1/d)).
 #include <algorithm>
+#include <climits>
 #include <cstdio>
 #include <cstdlib>
 #include <type_traits>
@@ -85,6 +86,15 @@ __device__ __forceinline__ float gt01(float a, float b) {
     asm("set.gt.f32.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
     return r;
 }
+
+// Segments of the direction-split fast loop: kSegSteps steps whose samples are
+// bounded together.  Per segment: the range of the forward DEM offsets (x, y)
+// over its steps, the largest and smallest 1/d and the largest filter offset.
+constexpr uint32_t kSegSteps = 32;
+struct __align__(16) SegBound {
+    int dx0, dx1, dy0, dy1;
+    float ymax, ymin, zmax, pad;
+};
 
 // One packed table entry: {y, y}, {-d, -d}, {d/R, d/R}, {d*tan1, d*tan1}.
 struct PackedStep {
@@ -215,8 +225,8 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
                                                  uint32_t by, uint32_t n, uint32_t n_fast,
                                                  const float4 *s_steps, const long long *s_boff,
                                                  const double *s_c64, const float *s_zf,
-                                                 const float &hmax, void *s_fwd_raw,
-                                                 Wait &&wait_prev) {
+                                                 const SegBound *s_seg, const float &hmax,
+                                                 void *s_fwd_raw, Wait &&wait_prev) {
     constexpr bool kMix = kPrec == TVS_PRECISION_MIXED64;
     using S = typename std::conditional<kMix, double, float>::type;  // surfaces
     constexpr int K = kSplitCols, KX = K / KY, LY = 32 / LX;
@@ -248,6 +258,43 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
             const long long b = s_boff[step];
             return (const float *)((const char *)ep[k / KX] + (dir ? -b : b)) + LX * (k % KX);
         };
+        // The largest elevation any lane of this warp samples in a segment: the
+        // block maxima over the warp's patch of points of view moved by the
+        // segment's offset range (warp-uniform).
+        auto segment_max = [&](const SegBound &b) -> float {
+            const int px0 = (int)(bx * (KX * LX) + D.los), px1 = px0 + KX * LX - 1;
+            const int py0 = (int)(D.row_begin + by * (kTileY * LY * KY) + threadIdx.y * LY * KY + D.los);
+            const int py1 = py0 + LY * KY - 1;
+            const int x0 = dir ? px0 - b.dx1 : px0 + b.dx0, x1 = dir ? px1 - b.dx0 : px1 + b.dx1;
+            const int y0 = dir ? py0 - b.dy1 : py0 + b.dy0, y1 = dir ? py1 - b.dy0 : py1 + b.dy1;
+            const int bx0 = max(x0, 0) / (int)kBlockMax;
+            const int bx1 = min(max(x1, 0) / (int)kBlockMax, (int)D.bmax_w - 1);
+            const int by0 = max(y0, 0) / (int)kBlockMax;
+            const int by1 = min(max(y1, 0) / (int)kBlockMax, (int)D.bmax_h - 1);
+            const int nx = bx1 - bx0 + 1, cells = nx > 0 && by1 >= by0 ? nx * (by1 - by0 + 1) : 0;
+            float m = -INFINITY;
+            for (int q = (int)threadIdx.x; q < cells; q += 32)
+                m = fmaxf(m, __ldg(D.bmax + (size_t)(by0 + q / nx) * D.bmax_w + bx0 + q % nx));
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+            return m;
+        };
+        // A segment can be skipped when no chain's filter can pass at any of its
+        // steps: with e <= RN(B - h_pov) for every sample, fma(e, y, z) at a step
+        // is at most fma(RN(B - h_pov), y_max or y_min, z_max) (RN and fma are
+        // monotone), so a bound below the chain's threshold rules the whole
+        // segment out exactly as the per-step filter would.
+        auto skippable = [&](uint32_t seg, auto &&lo_of) -> bool {
+            const SegBound b = s_seg[seg];
+            const float B = segment_max(b);
+            bool skip = true;
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const float E = __fsub_rn(B, hp32[k]);
+                skip &= __fmaf_rn(E, E >= 0.0f ? b.ymax : b.ymin, b.zmax) < lo_of(k);
+            }
+            return __all_sync(0xffffffffu, skip);
+        };
         S out[K];
         uint32_t i = 0;
         if constexpr (kMix) {
@@ -263,8 +310,14 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
             Chain<TVS_PRECISION_MIXED64> c[K];
 #pragma unroll
             for (int k = 0; k < K; k++) c[k].init();
+            for (uint32_t seg = 0; i < n_fast; seg++) {
+            const uint32_t i1 = min(i + kSegSteps, n_fast);
+            if (skippable(seg, [&](int k) { return c[k].lo; })) {
+                i = i1;
+                continue;
+            }
             TVS_UNROLL(TVS_SPLIT_UNROLL)
-            for (; i < n_fast; i++) {
+            for (; i < i1; i++) {
                 const float4 t = s_steps[i];
                 // filter (see the row layout): estimate + g >= m32 - gm
                 float e[K];
@@ -310,6 +363,7 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
                     }
                 }
             }
+            }
 #pragma unroll
             for (int k = 0; k < K; k++) c[k].m = max64(k, c[k].j);
             // the steps past the table-division domain (zero distances), IEEE division
@@ -340,8 +394,14 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
                 c[k].init();
                 lo[k] = exact_lo(c[k].m);
             }
+            for (uint32_t seg = 0; i < n_fast; seg++) {
+            const uint32_t i1 = min(i + kSegSteps, n_fast);
+            if (skippable(seg, [&](int k) { return lo[k]; })) {
+                i = i1;
+                continue;
+            }
             TVS_UNROLL(TVS_SPLIT_UNROLL)
-            for (; i < n_fast; i++) {
+            for (; i < i1; i++) {
                 const float4 t = s_steps[i];
                 const float zf = s_zf[i];
                 float e[K];
@@ -359,6 +419,7 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
                     c[k].m = fmaxf(ang, c[k].m);  // f32::max: NaN yields the other operand
                     lo[k] = exact_lo(c[k].m);
                 }
+            }
             }
             for (; i < n; i++) {
                 const float4 t = s_steps[i];
@@ -425,7 +486,8 @@ k_sweep_queue(QueueArgs a) {
     // exact f32: the filter offset), then the forward surfaces
     double *s_c64 = reinterpret_cast<double *>(s_boff + a.max_step_cap);
     float *s_zf = reinterpret_cast<float *>(s_boff + a.max_step_cap);
-    void *s_fwd = s_c64 + a.max_step_cap;
+    SegBound *s_seg = reinterpret_cast<SegBound *>(s_c64 + a.max_step_cap);
+    void *s_fwd = s_seg + (a.max_step_cap + kSegSteps - 1) / kSegSteps;
     const uint32_t tid = threadIdx.y * kTileX + threadIdx.x;
     const uint32_t n_items = a.tiles_per_sector * a.n_sectors;
     if (tid == 0) {
@@ -504,6 +566,36 @@ k_sweep_queue(QueueArgs a) {
                     s_pk[i] = p;
                 }
             }
+            if constexpr (kSplit) {
+                // segment bounds of the fast steps, one warp per segment
+                __syncthreads();
+                const uint32_t nf = h->n_fast, lane = threadIdx.x;
+                const long long W = D.width;
+                for (uint32_t sg = threadIdx.y; sg * kSegSteps < nf; sg += kTileY) {
+                    const uint32_t i = sg * kSegSteps + lane;
+                    const bool v = i < nf;
+                    // the step's forward offset as (x, y): |x| < W/2 on every band of sight
+                    const long long off = v ? s_boff[i] / (long long)sizeof(float) : 0;
+                    const long long q = off + W / 2;
+                    const long long dy = q >= 0 ? q / W : -((W - 1 - q) / W);
+                    const int dx = (int)(off - dy * W);
+                    int dx0 = v ? dx : INT_MAX, dx1 = v ? dx : INT_MIN;
+                    int dy0 = v ? (int)dy : INT_MAX, dy1 = v ? (int)dy : INT_MIN;
+                    float ymax = v ? s_steps[i].x : -INFINITY, ymin = v ? s_steps[i].x : INFINITY;
+                    float zmax = v ? (kMix ? s_steps[i].y : s_zf[i]) : -INFINITY;
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        dx0 = min(dx0, __shfl_xor_sync(0xffffffffu, dx0, o));
+                        dx1 = max(dx1, __shfl_xor_sync(0xffffffffu, dx1, o));
+                        dy0 = min(dy0, __shfl_xor_sync(0xffffffffu, dy0, o));
+                        dy1 = max(dy1, __shfl_xor_sync(0xffffffffu, dy1, o));
+                        ymax = fmaxf(ymax, __shfl_xor_sync(0xffffffffu, ymax, o));
+                        ymin = fminf(ymin, __shfl_xor_sync(0xffffffffu, ymin, o));
+                        zmax = fmaxf(zmax, __shfl_xor_sync(0xffffffffu, zmax, o));
+                    }
+                    if (lane == 0) s_seg[sg] = SegBound{dx0, dx1, dy0, dy1, ymax, ymin, zmax, 0.0f};
+                }
+            }
             if (tid == 0) {
                 ctl.sector_status = h->status;
                 ctl.n_steps = n;
@@ -545,7 +637,7 @@ k_sweep_queue(QueueArgs a) {
         if constexpr (kSplit) {
             if (run)
                 sweep_tile_split<kPrec, split_lx(kVar - 2), split_ky(kVar - 2)>(
-                    a, D, bx, by, n, n_fast, s_steps, s_boff, s_c64, s_zf, ctl.hmax, s_fwd,
+                    a, D, bx, by, n, n_fast, s_steps, s_boff, s_c64, s_zf, s_seg, ctl.hmax, s_fwd,
                     wait_prev);
         } else if (run) {
             const float *ep[kPy];
@@ -934,7 +1026,7 @@ QueueConfig default_queue_config(int precision) {
         if (f) d.prefetch = atoi(f) != 0;
         return d;
     }();
-    // MIXED64 defaults to layout 2 and exact f32 to layout 6 (the fastest on
+    // MIXED64 defaults to layout 2 and exact f32 to layout 5 (the fastest on
     // one B200 at 3601^2); TVS_SWEEP_LAYOUT and TVS_SWEEP_LAYOUT32 override them
     static const int split = [] {
         const char *l = getenv("TVS_SWEEP_LAYOUT");
@@ -942,7 +1034,7 @@ QueueConfig default_queue_config(int precision) {
     }();
     static const int split32 = [] {
         const char *l = getenv("TVS_SWEEP_LAYOUT32");
-        return l ? atoi(l) : 6;
+        return l ? atoi(l) : 5;
     }();
     const int l = precision == TVS_PRECISION_MIXED64 ? split
                   : precision == TVS_PRECISION_EXACT32 ? split32
@@ -986,6 +1078,7 @@ cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, const QueueCon
     const size_t smem =
         c.layout ? sizeof(QueueCtl) +
                        (size_t)a.max_step_cap * (sizeof(float4) + 2 * sizeof(long long)) +
+                       (size_t)(a.max_step_cap + kSegSteps - 1) / kSegSteps * sizeof(SegBound) +
                        (size_t)kThreads * kSplitCols * sizeof(double)
                  : sizeof(QueueCtl) +
                        (size_t)a.max_step_cap * (sizeof(float4) + sizeof(long long) + (wide ? 32 : 0));

@@ -32,6 +32,8 @@ struct tvs_context {
     uint32_t done_cap = 0;
     int32_t *d_error = nullptr;
     float *d_hmax = nullptr;  // max |elevation| + |observer height| (estimate windows)
+    float *d_bmax = nullptr;  // block maxima of the elevations (segment bounds)
+    uint32_t bmax_w = 0, bmax_h = 0;
     unsigned long long *d_rechecks = nullptr;  // MIXED64 FP64 re-decisions
     tvs::QueueDem *d_qdem = nullptr;           // this context as a one-DEM queue
     tvs::QueueConfig qcfg{0, 0, 0, 0, 0};            // sweep configuration (autotuned or default)

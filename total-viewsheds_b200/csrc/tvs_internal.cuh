@@ -21,6 +21,9 @@ namespace tvs {
 constexpr float kMaxAngle = -2000.0f;
 constexpr float kTanOneRad = 0.0174533f;
 constexpr float kEarthRadiusSquared = 12742000.0f;
+// Side of the DEM blocks whose maximum elevation bounds the direction-split
+// sweep's segments (kBlockMax x kBlockMax points per block).
+constexpr uint32_t kBlockMax = 16;
 
 #ifdef __CUDACC__
 // The FP64 sweep's per-step values from the step's f32 distance d
@@ -131,6 +134,8 @@ struct QueueDem {
     float *total;                      // nullable
     double *cumulative64;              // FP64/MIXED64 only
     const float *hmax;                 // MIXED64: max |elevation| + |observer height|
+    const float *bmax;                 // max elevation of each kBlockMax^2 block of the DEM
+    uint32_t bmax_w, bmax_h;           // blocks per row, block rows
     uint32_t tiles_x, tiles_y;         // set by queue_tile
     uint32_t tile_base;                // first item of this DEM within a sector
     uint32_t done_base;                // this DEM's per-tile counters in `done`
@@ -199,6 +204,10 @@ cudaError_t launch_ring_count(const uint32_t *rings, uint64_t bands, uint32_t re
 cudaError_t launch_ring_gather(const uint32_t *rings, uint64_t bands, uint32_t reserved,
                                const uint64_t *block_sums, const uint4 *spill, uint32_t n_spill,
                                uint64_t *offsets, uint32_t *ids, cudaStream_t s);
+// bmax[(y / kBlockMax) * bmax_w + x / kBlockMax] = max elevation of the block
+// (NaN ignored; -inf for an all-NaN block).
+cudaError_t launch_block_max(const float *elev, uint32_t width, uint32_t height, float *bmax,
+                             cudaStream_t s);
 cudaError_t launch_shape_tables(const ShapeArgs &a, uint32_t n_sectors, const int32_t *tab_deltas,
                                 const float *tab_dists, const unsigned char *installed,
                                 cudaStream_t s);
