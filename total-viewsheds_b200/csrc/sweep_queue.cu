@@ -210,9 +210,13 @@ __host__ __device__ constexpr int split_tile_h(int layout) {
     return kTileY * (32 / split_lx(layout)) * split_ky(layout);
 }
 
-// unroll factor of the direction-split fast loops (2: best of 1-4 on one B200)
+// unroll factors of the direction-split fast loops (exact f32: 2, the best of 1-4
+// on one B200; MIXED64: 1, which keeps its state within 64 registers)
 #ifndef TVS_SPLIT_UNROLL
 #define TVS_SPLIT_UNROLL 2
+#endif
+#ifndef TVS_SPLIT_UNROLL_MIX
+#define TVS_SPLIT_UNROLL_MIX 1
 #endif
 #define TVS_PRAGMA(x) _Pragma(#x)
 #define TVS_UNROLL(n) TVS_PRAGMA(unroll n)
@@ -308,15 +312,21 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
                 return j < 0 ? -2000.0 : exact_angle(k, (uint32_t)j);
             };
             Chain<TVS_PRECISION_MIXED64> c[K];
+            // the step of each chain's maximum lives in shared memory: it is
+            // written at every raise but read only on the rare re-decisions
+            int32_t *jk = reinterpret_cast<int32_t *>(reinterpret_cast<S *>(s_fwd_raw) + K * kThreads) + tid;
 #pragma unroll
-            for (int k = 0; k < K; k++) c[k].init();
+            for (int k = 0; k < K; k++) {
+                c[k].init();
+                jk[k * kThreads] = -1;
+            }
             for (uint32_t seg = 0; i < n_fast; seg++) {
             const uint32_t i1 = min(i + kSegSteps, n_fast);
             if (skippable(seg, [&](int k) { return c[k].lo; })) {
                 i = i1;
                 continue;
             }
-            TVS_UNROLL(TVS_SPLIT_UNROLL)
+            TVS_UNROLL(TVS_SPLIT_UNROLL_MIX)
             for (; i < i1; i++) {
                 const float4 t = s_steps[i];
                 // filter (see the row layout): estimate + g >= m32 - gm
@@ -341,7 +351,7 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
                     const bool am = fabsf(dd[k]) <= __fadd_rn(gw, c[k].gm);
                     if (!am && dd[k] > 0.0f) {  // surely visible
                         c[k].set_max32(ah[k], gw);
-                        c[k].j = (int32_t)i;
+                        jk[k * kThreads] = (int32_t)i;
                         c[k].s = __dadd_rn(c[k].s, w64);
                     }
                     any_amb |= am;
@@ -351,12 +361,13 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
                     // chain still has the state it was tested with
 #pragma unroll
                     for (int k = 0; k < K; k++) {
-                        if (c[k].j == (int32_t)i) continue;
+                        const int32_t jm = jk[k * kThreads];
+                        if (jm == (int32_t)i) continue;
                         if (!(fabsf(dd[k]) <= __fadd_rn(gw, c[k].gm))) continue;
                         if (a.rechecks) atomicAdd(a.rechecks, 1ull);
                         const double a64 = exact_angle(k, i);
-                        if (a64 > max64(k, c[k].j)) {
-                            c[k].j = (int32_t)i;
+                        if (a64 > max64(k, jm)) {
+                            jk[k * kThreads] = (int32_t)i;
                             c[k].set_max32(ah[k], gw);
                             c[k].s = __dadd_rn(c[k].s, w64);
                         }
@@ -365,7 +376,7 @@ __device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const Queue
             }
             }
 #pragma unroll
-            for (int k = 0; k < K; k++) c[k].m = max64(k, c[k].j);
+            for (int k = 0; k < K; k++) c[k].m = max64(k, jk[k * kThreads]);
             // the steps past the table-division domain (zero distances), IEEE division
             for (; i < n; i++) {
                 const float dist = s_steps[i].w;
@@ -1026,11 +1037,11 @@ QueueConfig default_queue_config(int precision) {
         if (f) d.prefetch = atoi(f) != 0;
         return d;
     }();
-    // MIXED64 defaults to layout 2 and exact f32 to layout 5 (the fastest on
+    // MIXED64 defaults to layout 1 and exact f32 to layout 5 (the fastest on
     // one B200 at 3601^2); TVS_SWEEP_LAYOUT and TVS_SWEEP_LAYOUT32 override them
     static const int split = [] {
         const char *l = getenv("TVS_SWEEP_LAYOUT");
-        return l ? atoi(l) : 2;
+        return l ? atoi(l) : 1;
     }();
     static const int split32 = [] {
         const char *l = getenv("TVS_SWEEP_LAYOUT32");
@@ -1079,7 +1090,7 @@ cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, const QueueCon
         c.layout ? sizeof(QueueCtl) +
                        (size_t)a.max_step_cap * (sizeof(float4) + 2 * sizeof(long long)) +
                        (size_t)(a.max_step_cap + kSegSteps - 1) / kSegSteps * sizeof(SegBound) +
-                       (size_t)kThreads * kSplitCols * sizeof(double)
+                       (size_t)kThreads * kSplitCols * (sizeof(double) + (mix ? sizeof(int32_t) : 0))
                  : sizeof(QueueCtl) +
                        (size_t)a.max_step_cap * (sizeof(float4) + sizeof(long long) + (wide ? 32 : 0));
 #define TVS_Q(X, Y)                                                                         \
