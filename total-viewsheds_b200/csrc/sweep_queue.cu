@@ -11,20 +11,28 @@
 //    when the sector changes.
 //  * A tile's sectors must be applied in order (the reference adds sector
 //    surfaces to each point's cumulative sum sector by sector, f32).  Each
-//    tile has a counter of completed sectors; the item (s, T) waits until the
-//    counter of T reaches s.  (s-1, T) was dequeued earlier by a CTA that is
-//    running, so the wait always ends; it is bounded anyway (spin limit ->
-//    TVS_ERR_TIMEOUT in the error word, the item is skipped, the run fails).
-//  * A thread sweeps kPx x kPy points of view: columns 32 apart share one
-//    address per step (load immediates), rows 8 apart share the table
-//    operands.  Forward and backward bands of a point of view run in the same
-//    loop; cum = (cum + forward) + backward keeps the reference's order.
-//  * Steps [0, n_fast) use the table division (Markstein, see sweep.cu) with
-//    no per-step test; the zero-distance tail uses IEEE division.
+//    tile has a counter of completed sectors; the item (s, T) waits, after
+//    its sweep and before its surface writes, until the counter of T reaches
+//    s.  (s-1, T) was dequeued earlier by a CTA that is running, so the wait
+//    always ends; it is bounded anyway (spin limit -> TVS_ERR_TIMEOUT in the
+//    error word, the item's writes are skipped, the run fails).
+//  * Row layouts: a thread sweeps kPx x kPy points of view (columns 32 apart
+//    share one address per step through load immediates, rows 8 apart share
+//    the table operands); forward and backward bands of a point of view run
+//    in the same loop; cum = (cum + forward) + backward keeps the reference's
+//    order.  Every step is evaluated.
+//  * Direction-split layouts (sweep_tile_split): a lane sweeps four points of
+//    view one direction at a time behind a warp-level filter (the exact
+//    arithmetic runs only where some chain may change state) and skips
+//    32-step segments that the DEM's block maxima rule out.
+//  * Steps [0, n_fast) use the table division (Markstein, see sweep.cu); the
+//    zero-distance tail uses IEEE division.
 //
-// Precision kPrec: TVS_PRECISION_EXACT32 (reference f32, bit-exact) or
+// Precision kPrec: TVS_PRECISION_EXACT32 (reference f32, bit-exact),
 // TVS_PRECISION_FP64 (the same control flow in double: angles, maximum and
-// surfaces; table division in double from y = RN64(1/d)).
+// surfaces; table division in double from y = RN64(1/d)) or
+// TVS_PRECISION_MIXED64 (FP32 estimates, FP64 decisions where the estimate is
+// ambiguous and FP64 surfaces: the FP64 results).
 #include <algorithm>
 #include <climits>
 #include <cstdio>
