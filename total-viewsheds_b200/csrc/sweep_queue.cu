@@ -99,6 +99,7 @@ __device__ __forceinline__ float gt01(float a, float b) {
 // bounded together.  Per segment: the range of the forward DEM offsets (x, y)
 // over its steps, the largest and smallest 1/d and the largest filter offset.
 constexpr uint32_t kSegSteps = 32;
+static_assert(kSegSteps == 32, "the staging reduces one segment per warp, one step per lane");
 struct __align__(16) SegBound {
     int dx0, dx1, dy0, dy1;
     float ymax, ymin, zmax, pad;
