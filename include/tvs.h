@@ -248,7 +248,7 @@ uint64_t tvs_device_bytes(const tvs_context *ctx);
  * holds LX = 8, 16, 32 (L = 1, 2, 3 and again 4, 5, 6) columns x 32/LX rows of
  * lanes; each lane has four points of view LX columns apart (L <= 3, tiles of
  * 4 LX x 256/LX points) or 2 x 2 of them, LX columns and 32/LX rows apart
- * (L >= 4, tiles of 2 LX x 512/LX).  Defaults: layout 1 for MIXED64, 5 for
+ * (L >= 4, tiles of 2 LX x 512/LX).  Defaults: layout 1 for MIXED64, 4 for
  * EXACT32, rows 2x1 for FP64.  Results do not depend on any of them. */
 typedef struct tvs_sweep_config {
     int32_t points_x;

@@ -79,7 +79,8 @@ def test_sweep_configurations_agree(tvs, synth, shape):
     assert np.array_equal(bits(want), bits(got)) and np.array_equal(bits(wt), bits(gt))
 
 
-@pytest.mark.parametrize("w,h,rows", [(301, 301, None), (311, 197, None), (301, 301, (37, 90))])
+@pytest.mark.parametrize("w,h,rows", [(301, 301, None), (311, 197, None), (301, 301, (37, 90)),
+                                      (301, 301, (40, 41))])
 @pytest.mark.parametrize("layout", [0, 1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("precision,reference", [("mixed64", "fp64"), ("exact32", "exact32")])
 def test_split_layouts_agree(tvs, synth, w, h, layout, rows, precision, reference):

@@ -98,8 +98,12 @@ __device__ __forceinline__ float gt01(float a, float b) {
 // Segments of the direction-split fast loop: kSegSteps steps whose samples are
 // bounded together.  Per segment: the range of the forward DEM offsets (x, y)
 // over its steps, the largest and smallest 1/d and the largest filter offset.
-constexpr uint32_t kSegSteps = 32;
-static_assert(kSegSteps == 32, "the staging reduces one segment per warp, one step per lane");
+#ifndef TVS_SEG_STEPS
+#define TVS_SEG_STEPS 32
+#endif
+constexpr uint32_t kSegSteps = TVS_SEG_STEPS;
+static_assert(kSegSteps >= 1 && kSegSteps <= 32,
+              "the staging reduces one segment per warp, one step per lane");
 struct __align__(16) SegBound {
     int dx0, dx1, dy0, dy1;
     float ymax, ymin, zmax, pad;
@@ -593,7 +597,7 @@ k_sweep_queue(QueueArgs a) {
                 const long long W = D.width;
                 for (uint32_t sg = threadIdx.y; sg * kSegSteps < nf; sg += kTileY) {
                     const uint32_t i = sg * kSegSteps + lane;
-                    const bool v = i < nf;
+                    const bool v = lane < kSegSteps && i < nf;
                     // the step's forward offset as (x, y): |x| < W/2 on every band of sight
                     const long long off = v ? s_boff[i] / (long long)sizeof(float) : 0;
                     const long long q = off + W / 2;
@@ -1017,8 +1021,13 @@ cudaError_t launch_queue_t(const QueueArgs &a, size_t smem, cudaStream_t s) {
 }  // namespace
 
 uint32_t queue_tiles_bound(uint32_t tvs_width, uint32_t rows) {
-    // the smallest tile (32 x 8 points) bounds the tile count of every shape
-    return ((tvs_width + kTileX - 1) / kTileX) * ((rows + kTileY - 1) / kTileY);
+    // the most tiles any configuration cuts: the row layouts' smallest tile is
+    // 32 x 8, but a split layout's tile can be narrower (16 x 64), which on a
+    // thin row shard gives more tiles
+    auto tiles = [&](uint32_t w, uint32_t h) { return ((tvs_width + w - 1) / w) * ((rows + h - 1) / h); };
+    uint32_t n = tiles(kTileX, kTileY);
+    for (int l = 1; l <= 6; l++) n = std::max(n, tiles(split_tile_w(l), split_tile_h(l)));
+    return n;
 }
 
 bool queue_config_valid(const QueueConfig &c) {
@@ -1046,7 +1055,7 @@ QueueConfig default_queue_config(int precision) {
         if (f) d.prefetch = atoi(f) != 0;
         return d;
     }();
-    // MIXED64 defaults to layout 1 and exact f32 to layout 5 (the fastest on
+    // MIXED64 defaults to layout 1 and exact f32 to layout 4 (the fastest on
     // one B200 at 3601^2); TVS_SWEEP_LAYOUT and TVS_SWEEP_LAYOUT32 override them
     static const int split = [] {
         const char *l = getenv("TVS_SWEEP_LAYOUT");
@@ -1054,7 +1063,7 @@ QueueConfig default_queue_config(int precision) {
     }();
     static const int split32 = [] {
         const char *l = getenv("TVS_SWEEP_LAYOUT32");
-        return l ? atoi(l) : 5;
+        return l ? atoi(l) : 4;
     }();
     const int l = precision == TVS_PRECISION_MIXED64 ? split
                   : precision == TVS_PRECISION_EXACT32 ? split32

@@ -23,7 +23,10 @@ constexpr float kTanOneRad = 0.0174533f;
 constexpr float kEarthRadiusSquared = 12742000.0f;
 // Side of the DEM blocks whose maximum elevation bounds the direction-split
 // sweep's segments (kBlockMax x kBlockMax points per block).
-constexpr uint32_t kBlockMax = 16;
+#ifndef TVS_BLOCK_MAX
+#define TVS_BLOCK_MAX 16
+#endif
+constexpr uint32_t kBlockMax = TVS_BLOCK_MAX;
 
 #ifdef __CUDACC__
 // The FP64 sweep's per-step values from the step's f32 distance d
