@@ -413,28 +413,22 @@ size_t shape_smem_bytes() {
 cudaError_t launch_shape_tables(const ShapeArgs &a, uint32_t n_sectors, const int32_t *tab_deltas,
                                 const float *tab_dists, const unsigned char *installed,
                                 cudaStream_t s) {
-    static bool configured = false;
+    // the attribute is set on every launch: it belongs to the current device
     const size_t smem = shape_smem_bytes();  // covers (bds + 2) * 8 + bds * 4 (host-checked)
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_shape_tables,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
+    cudaError_t e = cudaFuncSetAttribute(k_shape_tables, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
     if (n_sectors == 0) return cudaSuccess;
     k_shape_tables<<<n_sectors, kShapeThreads, smem, s>>>(a, tab_deltas, tab_dists, installed);
     return cudaGetLastError();
 }
 
 cudaError_t launch_shape(const ShapeArgs &a, uint32_t n_sectors, cudaStream_t s) {
-    static bool configured = false;
+    // the attribute is set on every launch: it belongs to the current device
     const size_t smem = shape_smem_bytes();
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_shape, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
+    cudaError_t e = cudaFuncSetAttribute(k_shape, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
     uint64_t rank_lo, rank_count;
     int axes_mode = a.sector_ids_out != nullptr;
     if (axes_mode) {
@@ -450,14 +444,11 @@ cudaError_t launch_shape(const ShapeArgs &a, uint32_t n_sectors, cudaStream_t s)
 
 cudaError_t launch_shape_batch(const ShapeArgs *d_args, uint32_t n_dems, uint32_t n_sectors,
                                cudaStream_t s) {
-    static bool configured = false;
+    // the attribute is set on every launch: it belongs to the current device
     const size_t smem = shape_smem_bytes();
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_shape_batch,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
+    cudaError_t e = cudaFuncSetAttribute(k_shape_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
     if (n_dems == 0 || n_sectors == 0) return cudaSuccess;
     k_shape_batch<<<n_dems * n_sectors, kShapeThreads, smem, s>>>(d_args, n_sectors);
     return cudaGetLastError();

@@ -36,6 +36,7 @@
 #include <algorithm>
 #include <climits>
 #include <cstdio>
+#include <mutex>
 #include <cstdlib>
 #include <type_traits>
 
@@ -994,19 +995,38 @@ k_sweep_queue(QueueArgs a) {
 template <int kPrec, int kPx, int kPy, int kVar>
 cudaError_t launch_queue_t(const QueueArgs &a, size_t smem, cudaStream_t s) {
     auto fn = k_sweep_queue<kPrec, kPx, kPy, kVar>;
-    static int blocks_per_sm = -1;
-    static size_t configured_smem = 0;
+    // the shared-memory attribute and the occupancy, per device (they belong to
+    // the device current at launch).  Contexts on several devices or host
+    // threads may launch this kernel concurrently, so the attribute only grows:
+    // a launch never finds it below its own shared memory.
+    struct Occupancy {
+        size_t attr = 0, smem = 0;
+        int blocks = -1;
+    };
+    static std::mutex mu;
+    static Occupancy occ[64];
     int dev = 0, sms = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    if (blocks_per_sm < 0 || configured_smem != smem) {
-        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, fn, kThreads, smem);
-        if (e != cudaSuccess) return e;
-        if (blocks_per_sm < 1) blocks_per_sm = 1;
-        configured_smem = smem;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    int blocks_per_sm;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        Occupancy &o = occ[dev];
+        if (smem > o.attr) {
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            o.attr = smem;
+        }
+        if (o.blocks < 0 || o.smem != smem) {
+            int b = 0;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreads, smem);
+            if (e != cudaSuccess) return e;
+            o.blocks = b < 1 ? 1 : b;
+            o.smem = smem;
+        }
+        blocks_per_sm = o.blocks;
     }
     if (a.done_total > a.done_cap) return cudaErrorInvalidValue;
     e = cudaMemsetAsync(a.queue, 0, sizeof(uint32_t), s);
