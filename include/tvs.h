@@ -301,11 +301,13 @@ uint64_t tvs_batch_device_bytes(const tvs_batch *batch);
  * account for every byte), and real-time callers that forbid allocation after
  * start-up because an allocation can block or fail at any moment.  Inputs and outputs are the caller's device pointers: d_elevations
  * (width*height f32), d_cumulative (in/out) and d_total (in/out, nullable),
- * computable_points_count f32 each.  The sector's intermediate tables live in
+ * computable_points_count f32 each, on device params->device (the call makes
+ * that device current and restores the caller's current device before it
+ * returns).  The sector's intermediate tables live in
  * a 64 KiB static device array inside the library (held by every GPU that
  * loads it, until exit); lines of sight longer than ~1590 cells do not fit and
  * return TVS_ERR_CAPACITY.  Exact f32 only.  The call is synchronous on
- * `stream` (a cudaStream_t, NULL for the legacy stream).  All calls share the
+ * `stream` (a cudaStream_t of that device, NULL for the legacy stream).  All calls share the
  * array and overlapping calls would race: the library serialises its own
  * calls.  The first call on a device looks up the array's device address:
  * make it before any stream capture.  Error text: tvs_last_error(NULL). */

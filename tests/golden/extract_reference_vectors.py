@@ -4,9 +4,10 @@ The reference (tombh/total-viewsheds, Rust) cannot be built in this
 environment (no cargo), so its unit tests cannot run.  Their expected values
 are the golden vectors that pin the oracle.  This script reads them, as text,
 from the reference sources and writes them to ``reference_vectors.json`` beside
-this file.  Run it where the reference checkout is present:
+this file.  Run it where a reference checkout is present, naming its root
+(the argument, or the TVS_REFERENCE_ROOT environment variable):
 
-    python tests/golden/extract_reference_vectors.py [REFERENCE_ROOT]
+    python tests/golden/extract_reference_vectors.py REFERENCE_ROOT
 
 Sources (paths inside the reference repository):
   crates/total-viewsheds/src/axes.rs:216-333         5x5 axes at 0 and 135 degrees
@@ -20,7 +21,6 @@ import re
 import sys
 from pathlib import Path
 
-DEFAULT_ROOT = Path("/root/reference")
 SRC = Path("crates/total-viewsheds/src")
 OUT = Path(__file__).resolve().parent / "reference_vectors.json"
 
@@ -133,4 +133,9 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else DEFAULT_ROOT)
+    import os
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TVS_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: extract_reference_vectors.py REFERENCE_ROOT "
+                 "(or set TVS_REFERENCE_ROOT)")
+    main(Path(root))

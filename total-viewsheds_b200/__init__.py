@@ -19,8 +19,7 @@ from pathlib import Path
 import numpy as np
 
 PKG = Path(__file__).resolve().parent
-# TVS_LIBRARY points at another build of the library (A/B comparisons of builds)
-LIB_PATH = Path(os.environ["TVS_LIBRARY"]) if os.environ.get("TVS_LIBRARY") else PKG / "libtvs_cuda.so"
+LIB_PATH = PKG / "libtvs_cuda.so"
 SECTOR_STEPS = 180
 
 OK = 0

@@ -19,8 +19,11 @@
 // and it keeps the last call's contents.  Calls that overlap on the GPU race
 // on it; this entry point keeps its own calls from overlapping by holding a
 // process-wide lock for the whole call and synchronising the stream before it
-// returns.  The first call on a device looks up the array's device address
-// (cudaGetSymbolAddress); make that first call before any stream capture.
+// returns.  The call runs on params->device: it makes that device current for
+// the call and gives the caller back the device that was current before.  The
+// first call on a device looks up the array's device address
+// (cudaGetSymbolAddress) with that device current; make that first call
+// before any stream capture.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -60,6 +63,21 @@ int fail(int code, const std::string &msg) {
 
 size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
 
+// Byte offsets of one sector's tables inside the scratch array.
+struct ScratchLayout {
+    size_t trig, hdr, steps, offs, dtab, deltas, dists, total;
+    ScratchLayout(uint32_t cap, uint32_t bds) {
+        trig = 0;
+        hdr = trig + align256(sizeof(tvs::SectorTrig));
+        steps = hdr + align256(sizeof(tvs::ShapeHeader));
+        offs = steps + align256((size_t)cap * sizeof(float4));
+        dtab = offs + align256((size_t)cap * sizeof(int2));
+        deltas = dtab + align256((size_t)cap * sizeof(double4));
+        dists = deltas + align256((size_t)bds * sizeof(int32_t));
+        total = dists + align256((size_t)bds * sizeof(float));
+    }
+};
+
 // Device address of the scratch array on the current device (looked up once
 // per device, on the first call made with that device current).
 int scratch_address(void **out) {
@@ -78,6 +96,10 @@ int scratch_address(void **out) {
     *out = g_scratch[dev];
     return TVS_OK;
 }
+
+int run_sector(const tvs_params *params, const tvs_geometry &g, uint32_t rb, uint32_t re,
+               uint32_t cap, const float *d_elevations, uint32_t angle, float *d_cumulative,
+               float *d_total, cudaStream_t s);
 
 }  // namespace
 
@@ -99,15 +121,8 @@ extern "C" int tvs_compute_sector_noalloc(const tvs_params *params, const float 
 
     // Layout of the scratch array for this geometry.
     const uint32_t cap = (g.band_steps_filled + 2 + 3) & ~3u;
-    const uint32_t bds = g.band_deltas_size;
-    const size_t off_trig = 0;
-    const size_t off_hdr = off_trig + align256(sizeof(tvs::SectorTrig));
-    const size_t off_steps = off_hdr + align256(sizeof(tvs::ShapeHeader));
-    const size_t off_offs = off_steps + align256((size_t)cap * sizeof(float4));
-    const size_t off_dtab = off_offs + align256((size_t)cap * sizeof(int2));
-    const size_t off_deltas = off_dtab + align256((size_t)cap * sizeof(double4));
-    const size_t off_dists = off_deltas + align256((size_t)bds * sizeof(int32_t));
-    const size_t total = off_dists + align256((size_t)bds * sizeof(float));
+    const ScratchLayout lay(cap, g.band_deltas_size);
+    const size_t total = lay.total;
     if (total > kScratchBytes) {
         char b[256];
         std::snprintf(b, sizeof b,
@@ -117,12 +132,41 @@ extern "C" int tvs_compute_sector_noalloc(const tvs_params *params, const float 
         return fail(TVS_ERR_CAPACITY, b);
     }
 
+    // Nothing to compute (a line of sight of exactly half the shorter side):
+    // no device work, as a context would do for the same geometry.
+    if (g.computable_points_count == 0 || rb == re) return TVS_OK;
+
     std::lock_guard<std::mutex> lock(g_mutex);
+    // The call runs on params->device (the device of the caller's buffers and
+    // stream) and gives the caller back the device that was current.
+    int previous = 0;
+    cudaError_t e = cudaGetDevice(&previous);
+    if (e != cudaSuccess)
+        return fail(TVS_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (params->device != previous && (e = cudaSetDevice(params->device)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(TVS_ERR_NO_DEVICE, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    }
+    rc = run_sector(params, g, rb, re, cap, d_elevations, angle, d_cumulative, d_total,
+                    static_cast<cudaStream_t>(stream));
+    if (params->device != previous) cudaSetDevice(previous);
+    return rc;
+}
+
+namespace {
+
+int run_sector(const tvs_params *params, const tvs_geometry &g, uint32_t rb, uint32_t re,
+               uint32_t cap, const float *d_elevations, uint32_t angle, float *d_cumulative,
+               float *d_total, cudaStream_t s) {
+    const uint32_t bds = g.band_deltas_size;
+    const ScratchLayout lay(cap, bds);
+    const size_t off_trig = lay.trig, off_hdr = lay.hdr, off_steps = lay.steps;
+    const size_t off_offs = lay.offs, off_dtab = lay.dtab, off_deltas = lay.deltas;
+    const size_t off_dists = lay.dists;
     void *base = nullptr;
-    rc = scratch_address(&base);
+    int rc = scratch_address(&base);
     if (rc) return rc;
     unsigned char *sc = static_cast<unsigned char *>(base);
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
 
     // axes.rs:95,127 angles (f32), glibc trigonometry as Rust std on linux-gnu.
     tvs::SectorTrig trig;
@@ -202,3 +246,5 @@ extern "C" int tvs_compute_sector_noalloc(const tvs_params *params, const float 
         return fail(TVS_ERR_CUDA, std::string("no-allocation sweep: ") + cudaGetErrorString(e));
     return TVS_OK;
 }
+
+}  // namespace

@@ -40,6 +40,9 @@
 // contract them into FMAs; the results are bit-identical to the reference.
 #include <cstdio>
 #include <cstdlib>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "tvs.h"
 #include "tvs_internal.cuh"
@@ -556,11 +559,28 @@ cudaError_t launch_sweep_engine(const SweepArgs &a, int precision, cudaStream_t 
         fn = rings ? k_sweep_exact32<true> : k_sweep_exact32<false>;
     else
         return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = grow_smem_attribute(reinterpret_cast<const void *>(fn), smem);
     if (e != cudaSuccess) return e;
     fn<<<grid, block, smem, s>>>(a);
     return cudaGetLastError();
+}
+
+cudaError_t grow_smem_attribute(const void *fn, size_t smem) {
+    // The attribute belongs to (kernel, device).  Host threads and contexts on
+    // several devices launch the same kernels with different line-of-sight
+    // lengths, so the attribute is only ever raised: a launch never finds it
+    // below the shared memory it asks for, whatever another thread set since.
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, size_t> attr;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t &cur = attr[std::make_pair(fn, dev)];
+    if (smem <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) cur = smem;
+    return e;
 }
 
 // Points of view per thread of the constant-table sweep: columns x rows.

@@ -218,6 +218,9 @@ cudaError_t launch_shape(const ShapeArgs &a, uint32_t n_sectors, cudaStream_t s)
 cudaError_t launch_sight_distances(const SectorTrig &t, uint32_t width, uint32_t height,
                                    float *out, cudaStream_t s);
 cudaError_t launch_sweep_engine(const SweepArgs &a, int precision, cudaStream_t s);
+// Raises kernel fn's dynamic shared-memory limit on the current device to at
+// least smem bytes (never lowers it; thread-safe).
+cudaError_t grow_smem_attribute(const void *fn, size_t smem);
 // One sector per launch with the step table staged in constant memory
 // (hdr/steps/offs point at that sector's tables; a.n_sectors must be 1).
 cudaError_t launch_sweep_const(const SweepArgs &a, int precision, uint32_t n_steps,
