@@ -236,6 +236,16 @@ uint64_t tvs_last_launch_count(const tvs_context *ctx);
  * added, the ring buffers on the first run that asks for ring records). */
 uint64_t tvs_device_bytes(const tvs_context *ctx);
 
+/* Failure detection of the persistent sweep (no counterpart in the reference,
+ * which has no device waits).  A work item waits for its tile's previous
+ * sector before adding its surfaces; the wait sleeps in steps of ~256 ns and
+ * gives up after spin_limit steps (0 = the default, about 2 s): the item's
+ * writes are skipped, later waits give up at once, and tvs_device_finish
+ * returns TVS_ERR_TIMEOUT.  held_tile (0xFFFFFFFF = none) is a test hook:
+ * that tile's completion counter never advances, so the wait of its next
+ * sector cannot be satisfied.  Applies to this context's later sweeps. */
+int tvs_set_queue_wait(tvs_context *ctx, uint32_t spin_limit, uint32_t held_tile);
+
 /* ---- sweep configuration and autotuning ------------------------------ */
 
 /* Points of view per thread of the persistent sweep: points_x columns 32

@@ -34,6 +34,26 @@ class OracleError(RuntimeError):
         self.code = code
 
 
+MODES = {"exact32": 0, "fp64": 1, "fp32": 2}
+
+
+class SweepOpts(ctypes.Structure):
+    _fields_ = [
+        ("mode", ctypes.c_int),
+        ("row_begin", ctypes.c_uint32),
+        ("row_end", ctypes.c_uint32),
+        ("cum32", ctypes.c_void_p),
+        ("cum64", ctypes.c_void_p),
+        ("rings", ctypes.c_void_p),
+        ("rings_len", ctypes.c_uint64),
+        ("counts", ctypes.c_void_p),
+        ("ids", ctypes.c_void_p),
+        ("ids_cap", ctypes.c_uint64),
+        ("ids_total", ctypes.c_void_p),
+        ("threads", ctypes.c_int),
+    ]
+
+
 class Geometry(ctypes.Structure):
     _fields_ = [
         ("width", ctypes.c_uint32),
@@ -87,6 +107,11 @@ def lib():
         L.tvso_run_f64.argtypes = [P(Geometry), ctypes.c_void_p, ctypes.c_float, ctypes.c_uint32,
                                    ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                    ctypes.c_int]
+        L.tvso_sweep_sector.argtypes = [P(Geometry), ctypes.c_void_p, ctypes.c_float,
+                                        ctypes.c_void_p, ctypes.c_void_p, P(SweepOpts)]
+        L.tvso_run_ex.argtypes = [P(Geometry), ctypes.c_void_p, ctypes.c_float, ctypes.c_uint32,
+                                  ctypes.c_uint32, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32,
+                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -183,6 +208,76 @@ def run_f64(g, elevations, observer_height, first_angle=0, n_angles=180, rings=F
     _check(lib().tvso_run_f64(ctypes.byref(g), _ptr(e), observer_height, first_angle,
                               n_angles, _ptr(cum), _ptr(r), threads or default_threads()))
     return cum, r
+
+
+def sweep_sector(g, elevations, observer_height, deltas, dists, mode="exact32", rows=None,
+                 cumulative=None, compact=False, threads=None):
+    """One sector in any mode over a row range (None = every row).
+
+    cumulative (f32, or f64 for mode "fp64"; [rows * tvs_width]) is advanced in
+    place (zeros when None).  Returns (cumulative, counts, ids): with
+    compact=True, counts (u32 [total_bands], 0 outside the rows) and the ids of
+    every band's ring record back to back in kernel-id order (the engine's
+    compact stream); otherwise (cumulative, None, None)."""
+    rb, re = (0, g.tvs_height) if rows is None else rows
+    n = (re - rb) * g.tvs_width
+    f64 = mode == "fp64"
+    if cumulative is None:
+        cumulative = np.zeros(n, np.float64 if f64 else np.float32)
+    assert cumulative.dtype == (np.float64 if f64 else np.float32) and cumulative.size == n
+    e = np.ascontiguousarray(elevations, np.float32)
+    o = SweepOpts()
+    o.mode = MODES[mode]
+    o.row_begin, o.row_end = rb, re
+    if f64:
+        o.cum64 = cumulative.ctypes.data
+    else:
+        o.cum32 = cumulative.ctypes.data
+    o.threads = threads or default_threads()
+    counts = ids = None
+    args = (ctypes.byref(g), _ptr(e), observer_height,
+            _ptr(np.ascontiguousarray(deltas, np.int32)),
+            _ptr(np.ascontiguousarray(dists, np.float32)))
+    if compact:
+        counts = np.zeros(g.total_bands, np.uint32)
+        total = ctypes.c_uint64(0)
+        saved = cumulative.copy()
+        cap = 24 * max(n, 1) * 2
+        ids = np.empty(cap, np.uint32)
+        o.counts, o.ids, o.ids_cap = counts.ctypes.data, ids.ctypes.data, cap
+        o.ids_total = ctypes.addressof(total)
+        _check(lib().tvso_sweep_sector(*args, ctypes.byref(o)))
+        if total.value > cap:  # the stream did not fit: once more with the exact size
+            cumulative[:] = saved
+            cap = total.value
+            ids = np.empty(cap, np.uint32)
+            o.ids, o.ids_cap = ids.ctypes.data, cap
+            _check(lib().tvso_sweep_sector(*args, ctypes.byref(o)))
+        ids = ids[:total.value]
+    else:
+        _check(lib().tvso_sweep_sector(*args, ctypes.byref(o)))
+    return cumulative, counts, ids
+
+
+def run_ex(g, elevations, observer_height, first_angle=0, n_angles=180, mode="exact32",
+           rows=None, threads=None):
+    """tvso_run over a row range in any mode: (cumulative, total or None)."""
+    rb, re = (0, 0) if rows is None else rows
+    nrows = (g.tvs_height if rows is None else re - rb)
+    n = nrows * g.tvs_width
+    e = np.ascontiguousarray(elevations, np.float32)
+    if mode == "fp64":
+        cum = np.empty(n, np.float64)
+        _check(lib().tvso_run_ex(ctypes.byref(g), _ptr(e), observer_height, first_angle,
+                                 n_angles, MODES[mode], rb, re, None, None, _ptr(cum),
+                                 threads or default_threads()))
+        return cum, None
+    cum = np.empty(n, np.float32)
+    total = np.empty(n, np.float32)
+    _check(lib().tvso_run_ex(ctypes.byref(g), _ptr(e), observer_height, first_angle, n_angles,
+                             MODES[mode], rb, re, _ptr(cum), _ptr(total), None,
+                             threads or default_threads()))
+    return cum, total
 
 
 def ascii_viewshed(g, pov_id, all_ring_data, reserved):

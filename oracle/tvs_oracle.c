@@ -398,6 +398,55 @@ static double sweep_band_f64(const tvso_geometry *g, uint64_t kernel_id,
     return band_surface;
 }
 
+/* The plain reciprocal-table FP32 form of kernel.rs:175 (the comparison
+ * baseline of the engine, not the reference's arithmetic): per step the tables
+ * y = RN(1/d), c = RN(d/12742000) and w = RN(d*0.0174533f) in f32, the angle
+ * fmaf(RN(h - h_pov), y, -c) (one rounding), f32 comparisons and f32 surface
+ * sums.  The control flow and the ring records are kernel.rs:153-243's. */
+static float sweep_band_fp32(const tvso_geometry *g, uint64_t kernel_id,
+                             const float *elev, float observer_height,
+                             const int32_t *deltas, const float *dists,
+                             band_out *o) {
+    uint64_t half_total_bands = g->total_bands / 2;
+    int forward = kernel_id < half_total_bands;
+    uint64_t tvs_id = forward ? kernel_id : kernel_id - half_total_bands;
+    uint64_t pov_x = tvs_id % g->tvs_width + g->max_los_as_points;
+    uint64_t pov_y = tvs_id / g->tvs_width + g->max_los_as_points;
+    int64_t pov_id = (int64_t)(pov_y * g->width + pov_x);
+    float pov_elevation = elev[pov_id] + observer_height;
+    float max_angle = MAX_ANGLE;
+    int is_currently_visible = 1, closing = 0, is_previously_visible = 1;
+    float band_surface = 0.0f;
+    uint32_t ring_id = 1;
+    o->ids[0] = (uint32_t)pov_id;
+    int64_t dem_id = pov_id;
+    o->status = TVSO_OK;
+    for (uint32_t i = 0; i < g->band_deltas_size; i++) {
+        int32_t delta = deltas[i];
+        dem_id = forward ? dem_id + delta : dem_id - delta;
+        if (dem_id < 0 || (uint64_t)dem_id >= g->size) {
+            o->status = TVSO_ERR_ELEVATION_OOB;
+            o->n_ids = ring_id;
+            return band_surface;
+        }
+        float distance = dists[i];
+        float y = 1.0f / distance;
+        float c = distance / EARTH_RADIUS_SQUARED;
+        float angle = fmaf(elev[dem_id] - pov_elevation, y, -c);
+        is_currently_visible = angle > max_angle;
+        int opening = is_currently_visible && !is_previously_visible;
+        closing = is_previously_visible && !is_currently_visible;
+        if (is_currently_visible) band_surface += distance * TAN_ONE_RAD;
+        if (opening) o->ids[ring_id++] = (uint32_t)dem_id;
+        if (closing) o->ids[ring_id++] = (uint32_t)dem_id;
+        is_previously_visible = is_currently_visible;
+        max_angle = fmaxf(angle, max_angle);
+    }
+    if (is_currently_visible && !closing) o->ids[ring_id++] = (uint32_t)dem_id;
+    o->n_ids = ring_id;
+    return band_surface;
+}
+
 /* kernel.rs:141-145,220-243,302-309: replay one band's ring writes into the
  * flat sector buffer in the reference's order (slot 1 .. n, then slot 0).
  * An index past the buffer is the reference's out-of-bounds panic. */
@@ -414,26 +463,41 @@ static int save_band_rings(uint64_t kernel_id, uint32_t reserved, const band_out
     return TVSO_OK;
 }
 
+/* One sector over the bands of computable rows [o->row_begin, o->row_end)
+ * (all rows when both are 0), forward bands before backward bands as
+ * compute.rs:229 orders them.  Surfaces go to o->cum32 / o->cum64 indexed from
+ * the first row of the range; ring records to the reference layout and/or the
+ * compact stream. */
 static int compute_sector_impl(const tvso_geometry *g, const float *elev,
                                float observer_height, const int32_t *deltas,
-                               const float *dists, float *cum32, double *cum64,
-                               uint32_t *rings, uint64_t rings_len, int threads) {
-    if (!g || !elev || !deltas || !dists) return TVSO_ERR_ARGS;
+                               const float *dists, const tvso_sweep_opts *opt) {
+    if (!g || !elev || !deltas || !dists || !opt) return TVSO_ERR_ARGS;
+    uint32_t rb = opt->row_begin, re = opt->row_end;
+    if (rb == 0 && re == 0) re = g->tvs_height;
+    if (rb > re || re > g->tvs_height) return TVSO_ERR_ARGS;
+    const int mode = opt->mode;
+    if (mode < TVSO_MODE_EXACT32 || mode > TVSO_MODE_FP32) return TVSO_ERR_ARGS;
+    const int f64 = mode == TVSO_MODE_F64;
+    if (f64 ? !opt->cum64 : !opt->cum32) return TVSO_ERR_ARGS;
     uint64_t half = g->total_bands / 2;
+    uint64_t t0 = (uint64_t)rb * g->tvs_width, t1 = (uint64_t)re * g->tvs_width;
+    uint64_t local = t1 - t0;
     uint32_t max_ids = g->band_deltas_size + 2;
-    /* Per tvs id: forward and backward surfaces and ring ids. */
+    /* Per tvs id of the range: forward and backward surfaces and ring ids. */
     float *sf32 = NULL, *sb32 = NULL;
     double *sf64 = NULL, *sb64 = NULL;
     band_out *outs = NULL;
     uint32_t *id_store = NULL;
+    uint64_t n_ids_total = 0;
     int rc = TVSO_ERR_NOMEM;
-    if (cum32) {
-        sf32 = malloc(half * sizeof(float));
-        sb32 = malloc(half * sizeof(float));
+    if (opt->counts) memset(opt->counts, 0, g->total_bands * sizeof(uint32_t));
+    if (!f64) {
+        sf32 = malloc((local ? local : 1) * sizeof(float));
+        sb32 = malloc((local ? local : 1) * sizeof(float));
         if (!sf32 || !sb32) goto done;
     } else {
-        sf64 = malloc(half * sizeof(double));
-        sb64 = malloc(half * sizeof(double));
+        sf64 = malloc((local ? local : 1) * sizeof(double));
+        sb64 = malloc((local ? local : 1) * sizeof(double));
         if (!sf64 || !sb64) goto done;
     }
     /* Bands are processed in blocks so the ring-id store stays bounded. */
@@ -443,52 +507,61 @@ static int compute_sector_impl(const tvso_geometry *g, const float *elev,
     if (!outs || !id_store) goto done;
     for (uint64_t j = 0; j < 2 * block; j++) outs[j].ids = id_store + j * max_ids;
 #ifdef _OPENMP
-    if (threads < 1) threads = 1;
+    int threads = opt->threads < 1 ? 1 : opt->threads;
     omp_set_num_threads(threads);
-#else
-    (void)threads;
 #endif
     rc = TVSO_OK;
     /* Forward bands (kernel ids 0..half) all run before the backward bands
      * (compute.rs:229): surfaces are added in that order below, and the ring
      * writes are replayed in kernel-id order. */
     for (int dir = 0; dir < 2 && rc == TVSO_OK; dir++) {
-        for (uint64_t b0 = 0; b0 < half && rc == TVSO_OK; b0 += block) {
-            uint64_t nb = half - b0 < block ? half - b0 : block;
+        for (uint64_t b0 = t0; b0 < t1 && rc == TVSO_OK; b0 += block) {
+            uint64_t nb = t1 - b0 < block ? t1 - b0 : block;
 #pragma omp parallel for schedule(static)
             for (int64_t j = 0; j < (int64_t)nb; j++) {
                 uint64_t tvs = b0 + (uint64_t)j;
                 uint64_t kid = dir == 0 ? tvs : tvs + half;
                 band_out *o = &outs[j];
-                if (cum32) {
-                    float s = sweep_band_f32(g, kid, elev, observer_height, deltas, dists, o);
-                    (dir == 0 ? sf32 : sb32)[tvs] = s;
+                if (f64) {
+                    double sv = sweep_band_f64(g, kid, elev, observer_height, deltas, dists, o);
+                    (dir == 0 ? sf64 : sb64)[tvs - t0] = sv;
                 } else {
-                    double s = sweep_band_f64(g, kid, elev, observer_height, deltas, dists, o);
-                    (dir == 0 ? sf64 : sb64)[tvs] = s;
+                    float sv = mode == TVSO_MODE_FP32
+                                   ? sweep_band_fp32(g, kid, elev, observer_height, deltas, dists, o)
+                                   : sweep_band_f32(g, kid, elev, observer_height, deltas, dists, o);
+                    (dir == 0 ? sf32 : sb32)[tvs - t0] = sv;
                 }
             }
             for (uint64_t j = 0; j < nb; j++) {
                 uint64_t tvs = b0 + j;
                 uint64_t kid = dir == 0 ? tvs : tvs + half;
                 if (outs[j].status != TVSO_OK) { rc = outs[j].status; break; }
-                if (rings) {
+                if (opt->rings) {
                     int r = save_band_rings(kid, g->reserved_rings_per_band, &outs[j],
-                                            rings, rings_len);
+                                            opt->rings, opt->rings_len);
                     if (r != TVSO_OK) { rc = r; break; }
+                }
+                if (opt->counts) {
+                    /* ids past ids_cap are counted, not copied: *ids_total > ids_cap
+                     * tells the caller that the stream was cut */
+                    opt->counts[kid] = outs[j].n_ids;
+                    if (opt->ids && n_ids_total + outs[j].n_ids <= opt->ids_cap)
+                        memcpy(opt->ids + n_ids_total, outs[j].ids, outs[j].n_ids * sizeof(uint32_t));
+                    n_ids_total += outs[j].n_ids;
                 }
             }
         }
     }
     if (rc != TVSO_OK) goto done;
+    if (opt->ids_total) *opt->ids_total = n_ids_total;
     /* kernel.rs:254: cumulative[tvs] += surface, forward band first. */
-    for (uint64_t t = 0; t < half; t++) {
-        if (cum32) {
-            cum32[t] += sf32[t];
-            cum32[t] += sb32[t];
+    for (uint64_t t = 0; t < local; t++) {
+        if (!f64) {
+            opt->cum32[t] += sf32[t];
+            opt->cum32[t] += sb32[t];
         } else {
-            cum64[t] += sf64[t];
-            cum64[t] += sb64[t];
+            opt->cum64[t] += sf64[t];
+            opt->cum64[t] += sb64[t];
         }
     }
 done:
@@ -496,13 +569,23 @@ done:
     return rc;
 }
 
+int tvso_sweep_sector(const tvso_geometry *g, const float *elevations, float observer_height,
+                      const int32_t *deltas, const float *dists, const tvso_sweep_opts *opts) {
+    return compute_sector_impl(g, elevations, observer_height, deltas, dists, opts);
+}
+
 int tvso_compute_sector(const tvso_geometry *g, const float *elevations,
                         float observer_height, const int32_t *deltas,
                         const float *dists, float *cumulative, uint32_t *rings,
                         uint64_t rings_len, int threads) {
     if (!cumulative) return TVSO_ERR_ARGS;
-    return compute_sector_impl(g, elevations, observer_height, deltas, dists,
-                               cumulative, NULL, rings, rings_len, threads);
+    tvso_sweep_opts o = {0};
+    o.mode = TVSO_MODE_EXACT32;
+    o.cum32 = cumulative;
+    o.rings = rings;
+    o.rings_len = rings_len;
+    o.threads = threads;
+    return compute_sector_impl(g, elevations, observer_height, deltas, dists, &o);
 }
 
 int tvso_compute_sector_f64(const tvso_geometry *g, const float *elevations,
@@ -510,15 +593,23 @@ int tvso_compute_sector_f64(const tvso_geometry *g, const float *elevations,
                             const float *dists, double *cumulative,
                             uint32_t *rings, uint64_t rings_len, int threads) {
     if (!cumulative) return TVSO_ERR_ARGS;
-    return compute_sector_impl(g, elevations, observer_height, deltas, dists,
-                               NULL, cumulative, rings, rings_len, threads);
+    tvso_sweep_opts o = {0};
+    o.mode = TVSO_MODE_F64;
+    o.cum64 = cumulative;
+    o.rings = rings;
+    o.rings_len = rings_len;
+    o.threads = threads;
+    return compute_sector_impl(g, elevations, observer_height, deltas, dists, &o);
 }
 
 static int run_impl(const tvso_geometry *g, const float *elev, float observer_height,
-                    uint32_t first_angle, uint32_t n_angles, float *cum32,
-                    float *total, double *cum64, uint32_t *rings_all, int threads) {
+                    uint32_t first_angle, uint32_t n_angles, int mode, uint32_t rb, uint32_t re,
+                    float *cum32, float *total, double *cum64, uint32_t *rings_all,
+                    int threads) {
     if (!g || !elev || first_angle + n_angles > SECTOR_STEPS) return TVSO_ERR_ARGS;
-    uint64_t count = g->computable_points_count;
+    if (rb == 0 && re == 0) re = g->tvs_height;
+    if (rb > re || re > g->tvs_height) return TVSO_ERR_ARGS;
+    uint64_t count = (uint64_t)(re - rb) * g->tvs_width;
     uint64_t ring_len = g->total_bands * (uint64_t)g->reserved_rings_per_band;
     int32_t *deltas = calloc(g->band_deltas_size ? g->band_deltas_size : 1, sizeof(int32_t));
     float *dists = calloc(g->band_deltas_size ? g->band_deltas_size : 1, sizeof(float));
@@ -532,9 +623,16 @@ static int run_impl(const tvso_geometry *g, const float *elev, float observer_he
         uint32_t angle = first_angle + a;
         rc = tvso_compile_band_data(g, (float)angle, deltas, dists, NULL);
         if (rc) break;
-        uint32_t *rings = rings_all ? rings_all + (uint64_t)a * ring_len : NULL;
-        rc = compute_sector_impl(g, elev, observer_height, deltas, dists, cum32, cum64,
-                                 rings, ring_len, threads);
+        tvso_sweep_opts o = {0};
+        o.mode = mode;
+        o.row_begin = rb;
+        o.row_end = re;
+        o.cum32 = cum32;
+        o.cum64 = cum64;
+        o.rings = rings_all ? rings_all + (uint64_t)a * ring_len : NULL;
+        o.rings_len = ring_len;
+        o.threads = threads;
+        rc = compute_sector_impl(g, elev, observer_height, deltas, dists, &o);
         if (rc) break;
         if (total && cum32)                                  /* compute.rs:206-214 */
             for (uint64_t t = 0; t < count; t++) total[t] += cum32[t];
@@ -548,14 +646,25 @@ int tvso_run(const tvso_geometry *g, const float *elevations, float observer_hei
              uint32_t first_angle, uint32_t n_angles, float *cumulative,
              float *total, uint32_t *rings_all, int threads) {
     if (!cumulative) return TVSO_ERR_ARGS;
-    return run_impl(g, elevations, observer_height, first_angle, n_angles, cumulative,
-                    total, NULL, rings_all, threads);
+    return run_impl(g, elevations, observer_height, first_angle, n_angles, TVSO_MODE_EXACT32,
+                    0, 0, cumulative, total, NULL, rings_all, threads);
 }
 
 int tvso_run_f64(const tvso_geometry *g, const float *elevations,
                  float observer_height, uint32_t first_angle, uint32_t n_angles,
                  double *cumulative, uint32_t *rings_all, int threads) {
     if (!cumulative) return TVSO_ERR_ARGS;
-    return run_impl(g, elevations, observer_height, first_angle, n_angles, NULL, NULL,
-                    cumulative, rings_all, threads);
+    return run_impl(g, elevations, observer_height, first_angle, n_angles, TVSO_MODE_F64,
+                    0, 0, NULL, NULL, cumulative, rings_all, threads);
+}
+
+int tvso_run_ex(const tvso_geometry *g, const float *elevations, float observer_height,
+                uint32_t first_angle, uint32_t n_angles, int mode, uint32_t row_begin,
+                uint32_t row_end, float *cumulative32, float *total, double *cumulative64,
+                int threads) {
+    if (mode == TVSO_MODE_F64 ? !cumulative64 : !cumulative32) return TVSO_ERR_ARGS;
+    return run_impl(g, elevations, observer_height, first_angle, n_angles, mode, row_begin,
+                    row_end, mode == TVSO_MODE_F64 ? NULL : cumulative32,
+                    mode == TVSO_MODE_F64 ? NULL : total,
+                    mode == TVSO_MODE_F64 ? cumulative64 : NULL, NULL, threads);
 }

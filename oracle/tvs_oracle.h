@@ -93,6 +93,32 @@ int tvso_compute_sector_f64(const tvso_geometry *g, const float *elevations,
                             const float *dists, double *cumulative,
                             uint32_t *rings, uint64_t rings_len, int threads);
 
+/* Sweep arithmetic of tvso_sweep_sector / tvso_run_ex. */
+#define TVSO_MODE_EXACT32 0   /* kernel.rs:164-233 in f32, the reference            */
+#define TVSO_MODE_F64 1       /* the same control flow in double                    */
+#define TVSO_MODE_FP32 2      /* reciprocal-table f32 form: fmaf(e, RN(1/d), -RN(d/R)) */
+
+typedef struct tvso_sweep_opts {
+    int mode;                      /* TVSO_MODE_*                                        */
+    uint32_t row_begin, row_end;   /* computable rows [begin, end); 0, 0 = every row     */
+    float *cum32;                  /* f32 modes: [rows * tvs_width] read-modify-written  */
+    double *cum64;                 /* TVSO_MODE_F64: [rows * tvs_width]                   */
+    uint32_t *rings;               /* reference layout (nullable, zeroed by the caller)  */
+    uint64_t rings_len;
+    uint32_t *counts;              /* compact records (nullable): ids per band, every   */
+                                   /* band of the sector (0 outside the row range)       */
+    uint32_t *ids;                 /* the bands' ids back to back, kernel-id order      */
+    uint64_t ids_cap;              /*   (nullable; needs counts)                          */
+    uint64_t *ids_total;           /* total ids of the records (nullable); when it is   */
+                                   /* above ids_cap, only the records that fit whole    */
+                                   /* before the cap were copied                         */
+    int threads;
+} tvso_sweep_opts;
+
+/* compute.rs:228-240 + kernel.rs:71-256 for one sector, with the options above. */
+int tvso_sweep_sector(const tvso_geometry *g, const float *elevations, float observer_height,
+                      const int32_t *deltas, const float *dists, const tvso_sweep_opts *opts);
+
 /* compute.rs:101-115,200-214: sectors first_angle .. first_angle+n_angles-1.
  * cumulative and total (heatmap running total) [computable] are zeroed here.
  * rings_all (nullable) receives n_angles * (total_bands * reserved) u32. */
@@ -103,6 +129,14 @@ int tvso_run(const tvso_geometry *g, const float *elevations, float observer_hei
 int tvso_run_f64(const tvso_geometry *g, const float *elevations,
                  float observer_height, uint32_t first_angle, uint32_t n_angles,
                  double *cumulative, uint32_t *rings_all, int threads);
+
+/* tvso_run over computable rows [row_begin, row_end) (0, 0 = all) in any mode:
+ * the surfaces of those rows only ([rows * tvs_width]); cumulative32 and total
+ * for the f32 modes, cumulative64 for TVSO_MODE_F64. */
+int tvso_run_ex(const tvso_geometry *g, const float *elevations, float observer_height,
+                uint32_t first_angle, uint32_t n_angles, int mode, uint32_t row_begin,
+                uint32_t row_end, float *cumulative32, float *total, double *cumulative64,
+                int threads);
 
 #ifdef __cplusplus
 }

@@ -130,3 +130,71 @@ def test_square_window_is_the_whole_dem(oracle):
         d, x, filled = oracle.compile_band_data(g, angle)
         assert filled == n
         assert np.array_equal(d, want_d) and np.array_equal(x.view(np.uint32), want_x.view(np.uint32))
+
+
+def test_compact_records_equal_the_reference_layout(oracle, synth):
+    """The compact stream (counts + ids back to back) holds exactly the ids each
+    band writes into its reserved slots (kernel.rs:141-145,220-243)."""
+    z = synth.fbm(121, 121, 0.75, 21, 0.0, 900.0)
+    g = oracle.geometry(121, 30.0, 1200, 60.0)
+    for angle in (0.0, 37.0, 90.0):
+        d, x, _ = oracle.compile_band_data(g, angle)
+        c0 = np.zeros(g.computable_points_count, np.float32)
+        r0 = np.zeros(oracle.ring_len(g), np.uint32)
+        oracle.compute_sector(g, z, 1.65, d, x, c0, r0)
+        c1, counts, ids = oracle.sweep_sector(g, z, 1.65, d, x, compact=True)
+        R = g.reserved_rings_per_band
+        rec = r0.reshape(-1, R)
+        assert np.array_equal(rec[:, 0], counts) and counts.max() < R
+        mask = np.arange(R - 1)[None, :] < counts[:, None]
+        assert np.array_equal(rec[:, 1:][mask], ids)
+        assert np.array_equal(c0.view(np.uint32), c1.view(np.uint32))
+
+
+@pytest.mark.parametrize("mode", ["exact32", "fp64", "fp32"])
+def test_row_ranges_are_slices_of_the_full_sweep(oracle, synth, mode):
+    z = synth.fbm(101, 101, 0.8, 23, 0.0, 600.0)
+    g = oracle.geometry(101, 10.0, 300)
+    full, full_total = oracle.run_ex(g, z, 1.65, 0, 20, mode)
+    for rows in [(0, 17), (17, 18), (18, g.tvs_height)]:
+        part, part_total = oracle.run_ex(g, z, 1.65, 0, 20, mode, rows=rows)
+        want = full.reshape(g.tvs_height, -1)[rows[0]:rows[1]].ravel()
+        assert np.array_equal(part, want), rows
+        if mode != "fp64":
+            want_t = full_total.reshape(g.tvs_height, -1)[rows[0]:rows[1]].ravel()
+            assert np.array_equal(part_total, want_t), rows
+
+
+def test_fp32_form_is_the_reciprocal_table_expression(oracle, synth):
+    """The FP32 comparison form evaluates fmaf(h - h_pov, RN(1/d), -RN(d/R)):
+    checked here on one band against a direct numpy restatement."""
+    z = synth.fbm(61, 61, 0.8, 29, 0.0, 400.0)
+    g = oracle.geometry(61, 10.0, 200)
+    d, x, n = oracle.compile_band_data(g, 23.0)
+    c, counts, ids = oracle.sweep_sector(g, z, 1.65, d, x, mode="fp32", rows=(0, 1),
+                                         compact=True)
+    # band 0 (forward), computed with numpy in f32 with one rounding for the fma
+    zf = z.astype(np.float32).ravel()
+    los = g.max_los_as_points
+    pov = los * 61 + los
+    hp = np.float32(zf[pov] + np.float32(1.65))
+    m, s, vis_prev, out = np.float32(-2000.0), np.float32(0.0), True, [pov]
+    dem = pov
+    for i in range(g.band_deltas_size):
+        dem += int(d[i])
+        e = np.float32(zf[dem] - hp)
+        dist = np.float32(x[i])
+        with np.errstate(divide="ignore", invalid="ignore"):
+            y = np.float32(np.float32(1.0) / dist)
+            cc = np.float32(dist / np.float32(12742000.0))
+            a = np.float32(np.float64(e) * np.float64(y) - np.float64(cc))  # exact product
+        vis = bool(a > m)
+        if vis:
+            s = np.float32(s + np.float32(dist * np.float32(0.0174533)))
+        if vis != vis_prev:
+            out.append(dem)
+        vis_prev = vis
+        m = a if np.isnan(m) else (m if np.isnan(a) else max(a, m))
+    if vis_prev:
+        out.append(dem)
+    assert counts[0] == len(out) and list(ids[:counts[0]]) == out

@@ -1,7 +1,7 @@
-"""The multi-rank path on CPU: two gloo ranks split a DEM's computable rows,
-compute them (here with the oracle, the test's stand-in for each rank's GPU),
-gather them, and reproduce the single-process result bit for bit; timings
-reduce to the max over ranks."""
+"""The multi-rank path on CPU: gloo ranks split a DEM's computable rows, each
+computes only its own rows (here with the oracle's row-range sweep, the
+test's stand-in for each rank's GPU), the rows are gathered, and the result is
+the single-process run bit for bit; timings reduce to the max over ranks."""
 
 import os
 import socket
@@ -41,25 +41,29 @@ def _rank(rank, world, port, z, out_dir):
         import total_viewsheds_b200.sharding as sh
         oracle = load_oracle()
         g = oracle.geometry(61, 5.0, 100)
-        cum, _, _ = oracle.run(g, z, 1.65, 0, 24, threads=1)
         b, e = sh.shard_rows(g.tvs_height, rank, world)
-        mine = cum.reshape(g.tvs_height, g.tvs_width)[b:e].ravel()
+        mine, mine_total = oracle.run_ex(g, z, 1.65, 0, 24, rows=(b, e), threads=1)
+        assert mine.size == (e - b) * g.tvs_width
         full = sh.gather_rows(mine, g.tvs_width, g.tvs_height, world)
+        full_total = sh.gather_rows(mine_total, g.tvs_width, g.tvs_height, world)
         t = sh.max_over_ranks(1.0 + rank)
         if rank == 0:
             np.save(os.path.join(out_dir, "full.npy"), full)
+            np.save(os.path.join(out_dir, "total.npy"), full_total)
             np.save(os.path.join(out_dir, "tmax.npy"), np.array([t]))
     finally:
         dist.destroy_process_group()
 
 
-def test_two_gloo_ranks_reassemble(synth, oracle, tmp_path):
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_compute_their_rows_and_reassemble(synth, oracle, tmp_path, world):
     z = synth.fbm(61, 61, 0.8, 5, 0.0, 300.0)
-    world = 2
     mp.start_processes(_rank, args=(world, _free_port(), z, str(tmp_path)), nprocs=world,
                        join=True, start_method="spawn")
     g = oracle.geometry(61, 5.0, 100)
-    want, _, _ = oracle.run(g, z, 1.65, 0, 24, threads=1)
+    want, want_total, _ = oracle.run(g, z, 1.65, 0, 24, threads=1)
     full = np.load(tmp_path / "full.npy")
     assert np.array_equal(full.view(np.uint32), want.view(np.uint32))
-    assert float(np.load(tmp_path / "tmax.npy")[0]) == 2.0
+    assert np.array_equal(np.load(tmp_path / "total.npy").view(np.uint32),
+                          want_total.view(np.uint32))
+    assert float(np.load(tmp_path / "tmax.npy")[0]) == float(world)

@@ -134,6 +134,7 @@ SIGNATURES = {
     "tvs_read_surfaces": (_INT, [_VP, _VP, _VP]),
     "tvs_device_cumulative": (_VP, [_VP]),
     "tvs_read_rechecks": (_INT, [_VP, _P(_U64), _INT]),
+    "tvs_set_queue_wait": (_INT, [_VP, _U32, _U32]),
     "tvs_stream": (_VP, [_VP]),
     "tvs_last_launch_count": (_U64, [_VP]),
     "tvs_device_bytes": (_U64, [_VP]),
@@ -384,6 +385,12 @@ class Engine:
         c = SweepConfig()
         self._check(lib().tvs_autotune(self.ctx, sample_sectors, ctypes.byref(c)))
         return c
+
+    def set_queue_wait(self, spin_limit=0, held_tile=None):
+        """The sweep's dependency-wait limit (0 = default) and, for failure
+        tests, a tile whose completion is never signalled."""
+        self._check(lib().tvs_set_queue_wait(self.ctx, spin_limit,
+                                             0xFFFFFFFF if held_tile is None else held_tile))
 
     def read_rechecks(self, reset=True):
         """MIXED64: comparisons re-decided in FP64 since the last reset."""

@@ -90,7 +90,8 @@ tvs::QueueArgs queue_args(const tvs_batch *b, uint32_t first, uint32_t count) {
     q.done_total = b->tiles_per_sector;
     q.done_cap = b->done_cap;
     q.error = b->d_error;
-    q.spin_limit = 1u << 23;
+    q.spin_limit = tvs::kDefaultSpinLimit;
+    q.held_tile = 0xFFFFFFFFu;
     q.rechecks = b->d_rechecks;
     return q;
 }

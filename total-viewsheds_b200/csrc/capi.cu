@@ -371,7 +371,8 @@ int enqueue_sweep(tvs_context *c, uint32_t first, uint32_t count, bool rings) {
         q.done_total = c->q_tiles_per_sector;
         q.done_cap = c->done_cap;
         q.error = c->d_error;
-        q.spin_limit = 1u << 23;  // ~2-4 s of 256 ns sleeps; a real wait is one item (~1 ms)
+        q.spin_limit = c->spin_limit;
+        q.held_tile = c->held_tile;
         q.rechecks = c->d_rechecks;
         TVS_CUDA(c, tvs::launch_sweep_queue(q, (int)c->p.precision, c->qcfg, c->stream));
         c->launches++;
@@ -1005,6 +1006,13 @@ int tvs_autotune(tvs_context *ctx, uint32_t sample_sectors, tvs_sweep_config *ch
     for (bool &p : ctx->pending) p = false;
     if (rc) return rc;
     if (chosen) tvs_get_sweep_config(ctx, chosen);
+    return TVS_OK;
+}
+
+int tvs_set_queue_wait(tvs_context *ctx, uint32_t spin_limit, uint32_t held_tile) {
+    if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
+    ctx->spin_limit = spin_limit ? spin_limit : tvs::kDefaultSpinLimit;
+    ctx->held_tile = held_tile;
     return TVS_OK;
 }
 

@@ -988,7 +988,7 @@ k_sweep_queue(QueueArgs a) {
         }
         __threadfence();   // this thread's surface writes before the tile's counter
         __syncthreads();
-        if (tid == 0) atomicAdd(a.done + D.done_base + tile, 1u);
+        if (tid == 0 && D.done_base + tile != a.held_tile) atomicAdd(a.done + D.done_base + tile, 1u);
     }
 }
 

@@ -39,6 +39,8 @@ struct tvs_context {
     tvs::QueueConfig qcfg{0, 0, 0, 0, 0};            // sweep configuration (autotuned or default)
     tvs::QueueConfig qcfg_uploaded{0, 0, 0, 0, 0};   // the tiling currently in d_qdem
     uint32_t q_tiles_per_sector = 0;
+    uint32_t spin_limit = tvs::kDefaultSpinLimit;  // dependency-wait iteration limit
+    uint32_t held_tile = 0xFFFFFFFFu;               // failure-detection test hook
     int32_t *d_deltas = nullptr;
     float *d_dists = nullptr;
     // ring output (allocated on first use)

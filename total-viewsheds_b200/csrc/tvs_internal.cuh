@@ -37,6 +37,10 @@ __device__ __forceinline__ double4 fp64_step(float d) {
     return make_double4(__drcp_rn(dd), __ddiv_rn(dd, 12742000.0), __dmul_rn(dd, 0.0174533), dd);
 }
 #endif
+// Iterations (256 ns sleeps) a work-queue dependency wait may take before it
+// gives up with TVS_ERR_TIMEOUT: about 2-4 s, against a real wait of one
+// work item (about a millisecond).
+constexpr uint32_t kDefaultSpinLimit = 1u << 23;
 constexpr float kSectorShift = 0.001f;
 constexpr uint32_t kSectorSteps = 180;
 
@@ -155,6 +159,9 @@ struct QueueArgs {
     uint32_t done_total, done_cap;
     int32_t *error;                    // TVS_ERR_TIMEOUT when a wait gives up
     uint32_t spin_limit;
+    uint32_t held_tile;                // failure-detection test hook: this tile
+                                       // counter (done_base + tile) never advances
+                                       // (0xFFFFFFFF: none)
     unsigned long long *rechecks;      // MIXED64: FP64 re-decisions (nullable)
 };
 
