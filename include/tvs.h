@@ -58,7 +58,12 @@ enum tvs_precision {
      * the all-FP64 sweep; surfaces accumulate in FP64. */
     TVS_PRECISION_MIXED64 = 1,
     /* The all-FP64 sweep (angles, running maximum, surfaces in double). */
-    TVS_PRECISION_FP64 = 2
+    TVS_PRECISION_FP64 = 2,
+    /* The plain reciprocal-table FP32 form, the comparison baseline (no
+     * counterpart in the reference): angle = fma(h - h_pov, RN(1/d), -RN(d/R))
+     * in one rounding, f32 comparisons and surfaces.  Its visibility differs
+     * from both the reference's f32 and from FP64 near ties. */
+    TVS_PRECISION_FP32 = 3
 };
 
 /* Which sweep kernel runs. */
@@ -218,6 +223,17 @@ int tvs_device_run_sectors(tvs_context *ctx, uint32_t first_angle, uint32_t coun
  * the shape stage (one CTA per sector) and the sweep (one launch). */
 int tvs_device_shape_sectors(tvs_context *ctx, uint32_t first_angle, uint32_t count);
 int tvs_device_sweep_sectors(tvs_context *ctx, uint32_t first_angle, uint32_t count);
+/* One whole total viewshed on the context's stream: zero the surfaces, the
+ * shape stage of all 180 sectors and one persistent sweep over them.  The
+ * first call runs these as plain launches and captures them in a CUDA graph;
+ * later calls replay the graph (one launch).  A new sweep configuration,
+ * installed shapes, wait settings or counters drop the graph.  No counterpart
+ * in the reference (its Compute::run loops sectors on the host,
+ * compute.rs:101-115). */
+int tvs_device_run_tvs(tvs_context *ctx);
+/* Device times of the last tvs_device_run_tvs: the reset and shape stage, and
+ * the sweep (waits for it to finish). */
+int tvs_last_run_times(tvs_context *ctx, float *shape_ms, float *sweep_ms);
 /* Wait for the stream and report the first error of the sectors enqueued
  * since the last tvs_device_finish, if any. */
 int tvs_device_finish(tvs_context *ctx);
@@ -245,6 +261,14 @@ uint64_t tvs_device_bytes(const tvs_context *ctx);
  * that tile's completion counter never advances, so the wait of its next
  * sector cannot be satisfied.  Applies to this context's later sweeps. */
 int tvs_set_queue_wait(tvs_context *ctx, uint32_t spin_limit, uint32_t held_tile);
+
+/* Sweep counters of the direction-split layouts, for roofline accounting (no
+ * counterpart in the reference).  enable != 0 zeroes them and counts the
+ * later sweeps; read gives [0] warp-steps swept (not skipped by the segment
+ * bounds), [1] warp-steps that passed the first test, [2] warp-steps of the
+ * table-division loop in all (swept or skipped), [3] 0. */
+int tvs_set_sweep_counters(tvs_context *ctx, int enable);
+int tvs_read_sweep_counters(tvs_context *ctx, uint64_t *counters);
 
 /* ---- sweep configuration and autotuning ------------------------------ */
 
@@ -335,6 +359,11 @@ int tvs_selftest_division(int32_t device, uint64_t n, uint64_t seed, uint64_t *m
 /* FP32 issue-rate microbenchmark (independent FFMA chains on every SM):
  * measured FP32 lane-instructions per second, the sweep's roofline peak. */
 int tvs_measure_fp32_issue(int32_t device, double *instructions_per_second);
+
+/* L1 load-throughput microbenchmark (every warp loading 32 consecutive
+ * floats, the sweep's access, from L1-resident data on every SM): bytes per
+ * second, the sweep's secondary roofline peak. */
+int tvs_measure_l1_load(int32_t device, double *bytes_per_second);
 
 #ifdef __cplusplus
 }

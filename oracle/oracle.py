@@ -211,14 +211,15 @@ def run_f64(g, elevations, observer_height, first_angle=0, n_angles=180, rings=F
 
 
 def sweep_sector(g, elevations, observer_height, deltas, dists, mode="exact32", rows=None,
-                 cumulative=None, compact=False, threads=None):
+                 cumulative=None, compact=False, rings=None, threads=None):
     """One sector in any mode over a row range (None = every row).
 
     cumulative (f32, or f64 for mode "fp64"; [rows * tvs_width]) is advanced in
     place (zeros when None).  Returns (cumulative, counts, ids): with
     compact=True, counts (u32 [total_bands], 0 outside the rows) and the ids of
     every band's ring record back to back in kernel-id order (the engine's
-    compact stream); otherwise (cumulative, None, None)."""
+    compact stream); otherwise (cumulative, None, None).  rings (zeroed u32
+    [total_bands * reserved], nullable) receives the reference's layout."""
     rb, re = (0, g.tvs_height) if rows is None else rows
     n = (re - rb) * g.tvs_width
     f64 = mode == "fp64"
@@ -234,6 +235,9 @@ def sweep_sector(g, elevations, observer_height, deltas, dists, mode="exact32", 
     else:
         o.cum32 = cumulative.ctypes.data
     o.threads = threads or default_threads()
+    if rings is not None:
+        assert rings.dtype == np.uint32 and not compact
+        o.rings, o.rings_len = rings.ctypes.data, rings.size
     counts = ids = None
     args = (ctypes.byref(g), _ptr(e), observer_height,
             _ptr(np.ascontiguousarray(deltas, np.int32)),

@@ -34,7 +34,7 @@ ERR_OUT_OF_MEMORY = -8
 ERR_CAPACITY = -9
 ERR_TIMEOUT = -10
 
-PRECISION = {"exact32": 0, "mixed64": 1, "fp64": 2}
+PRECISION = {"exact32": 0, "mixed64": 1, "fp64": 2, "fp32": 3}
 SWEEP_KERNEL = {"engine": 0, "plain": 1}
 
 
@@ -135,6 +135,11 @@ SIGNATURES = {
     "tvs_device_cumulative": (_VP, [_VP]),
     "tvs_read_rechecks": (_INT, [_VP, _P(_U64), _INT]),
     "tvs_set_queue_wait": (_INT, [_VP, _U32, _U32]),
+    "tvs_set_sweep_counters": (_INT, [_VP, _INT]),
+    "tvs_read_sweep_counters": (_INT, [_VP, _P(_U64)]),
+    "tvs_device_run_tvs": (_INT, [_VP]),
+    "tvs_last_run_times": (_INT, [_VP, _P(ctypes.c_float), _P(ctypes.c_float)]),
+    "tvs_measure_l1_load": (_INT, [_I32, _P(ctypes.c_double)]),
     "tvs_stream": (_VP, [_VP]),
     "tvs_last_launch_count": (_U64, [_VP]),
     "tvs_device_bytes": (_U64, [_VP]),
@@ -359,6 +364,26 @@ class Engine:
     def device_sweep_sectors(self, first=0, count=SECTOR_STEPS):
         self._check(lib().tvs_device_sweep_sectors(self.ctx, first, count))
 
+    def device_run_tvs(self):
+        """Zero the surfaces and enqueue all 180 sectors (one graph replay
+        after the first call)."""
+        self._check(lib().tvs_device_run_tvs(self.ctx))
+
+    def last_run_times(self):
+        """(shape-stage ms, sweep ms) of the last device_run_tvs."""
+        a, b = ctypes.c_float(), ctypes.c_float()
+        self._check(lib().tvs_last_run_times(self.ctx, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def sweep_counters(self, enable=None):
+        """Read the direction-split sweep counters ([swept, passed, all, 0]
+        warp-steps); enable=True/False first zeroes them and turns counting on/off."""
+        if enable is not None:
+            self._check(lib().tvs_set_sweep_counters(self.ctx, 1 if enable else 0))
+        v = (ctypes.c_uint64 * 4)()
+        self._check(lib().tvs_read_sweep_counters(self.ctx, v))
+        return list(v)
+
     def device_finish(self):
         self._check(lib().tvs_device_finish(self.ctx))
 
@@ -487,6 +512,15 @@ class Batch:
 def selftest_division(n, seed=0, device=0):
     out = ctypes.c_uint64()
     rc = lib().tvs_selftest_division(device, n, seed, ctypes.byref(out))
+    if rc:
+        _raise(rc)
+    return out.value
+
+
+def measure_l1_load(device=0):
+    """Measured L1 load bytes per second on `device` (32-float warp loads)."""
+    out = ctypes.c_double()
+    rc = lib().tvs_measure_l1_load(device, ctypes.byref(out))
     if rc:
         _raise(rc)
     return out.value

@@ -19,8 +19,8 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libtvs_cuda.so"
 CLI = PKG / "tvs"
-SOURCES = ["capi.cu", "shape.cu", "sweep.cu", "sweep_queue.cu", "noalloc.cu", "batch.cu",
-           "shape_cache.cu", "rings_compact.cu"]
+SOURCES = ["capi.cu", "shape.cu", "sweep.cu", "sweep_queue.cu", "sweep_split.cu", "noalloc.cu",
+           "batch.cu", "shape_cache.cu", "rings_compact.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -219,6 +219,8 @@ int tvs_batch_set_sweep_config(tvs_batch *b, const tvs_sweep_config *cfg) {
         return bfail(b, TVS_ERR_INVALID_ARGUMENT, "unsupported points-per-thread shape");
     if (c.layout != 0 && b->precision == TVS_PRECISION_FP64)
         return bfail(b, TVS_ERR_INVALID_ARGUMENT, "sweep layouts 1-6 are not available for FP64");
+    if (c.layout == 0 && b->precision == TVS_PRECISION_FP32)
+        return bfail(b, TVS_ERR_INVALID_ARGUMENT, "the FP32 form runs on sweep layouts 1-6 only");
     if (c.px != b->cfg.px || c.py != b->cfg.py || c.packed != b->cfg.packed ||
         c.prefetch != b->cfg.prefetch || c.layout != b->cfg.layout) {
         b->cfg = c;
@@ -245,6 +247,7 @@ int tvs_batch_autotune(tvs_batch *b, uint32_t sample_sectors, tvs_sweep_config *
     TVS_BCUDA(b, cudaSetDevice(b->device));
     const bool exact = b->precision == TVS_PRECISION_EXACT32;
     const bool f64 = b->precision == TVS_PRECISION_FP64;
+    const bool fp32 = b->precision == TVS_PRECISION_FP32;
     const tvs::QueueConfig cands[] = {{1, 1, 0, 0, 0}, {2, 1, 0, 0, 0}, {4, 1, 0, 0, 0},
                                       {2, 2, 0, 0, 0}, {2, 1, 1, 0, 0}, {4, 1, 1, 0, 0},
                                       {1, 1, 0, 1, 0}, {2, 1, 0, 1, 0}, {4, 1, 0, 1, 0},
@@ -258,7 +261,7 @@ int tvs_batch_autotune(tvs_batch *b, uint32_t sample_sectors, tvs_sweep_config *
     tvs::QueueConfig best_cfg = b->cfg;
     int rc = TVS_OK;
     for (const tvs::QueueConfig &c : cands) {
-        if ((c.packed && !exact) || (c.layout != 0 && f64)) continue;
+        if ((c.packed && !exact) || (c.layout != 0 && f64) || (c.layout == 0 && fp32)) continue;
         tvs_sweep_config sc{c.px, c.py, c.packed, c.prefetch, c.layout};
         if ((rc = tvs_batch_set_sweep_config(b, &sc))) break;
         float ms = 0.0f;

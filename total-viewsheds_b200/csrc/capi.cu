@@ -21,6 +21,9 @@ thread_local std::string g_create_error;
 constexpr double kRadsPerDeg = 3.14159265358979323846 / 180.0;  // Rust f64::to_radians
 constexpr double kSqrt2 = 1.41421356237309504880;               // core::f64::consts::SQRT_2
 constexpr uint32_t kSpillCap = 1u << 20;
+// Slots per band of the device buffer behind the compact ring stream: a band
+// with more ids puts the rest in the spill list (rare at this size).
+constexpr uint32_t kCompactSlots = 64;
 
 int fail(tvs_context *ctx, int code, const std::string &msg) {
     if (ctx) ctx->err = msg; else g_create_error = msg;
@@ -131,15 +134,28 @@ int derive_geometry(const tvs_params *p, tvs_geometry *g, std::string *msg) {
     return TVS_OK;
 }
 
+// The captured whole-TVS graph depends on the sweep configuration, the
+// installed shapes, the wait settings and the counters: any change drops it.
+void drop_tvs_graph(tvs_context *c) {
+    if (c->tvs_exec) cudaGraphExecDestroy(c->tvs_exec);
+    if (c->tvs_graph) cudaGraphDestroy(c->tvs_graph);
+    c->tvs_exec = nullptr;
+    c->tvs_graph = nullptr;
+}
+
 void free_all(tvs_context *c) {
     void *ptrs[] = {c->d_elev, c->d_cum, c->d_total, c->d_cum64, c->d_trig, c->d_hdr,
                     c->d_steps, c->d_offs, c->d_dtab, c->d_queue, c->d_done, c->d_error, c->d_hmax,
                     c->d_rechecks, c->d_qdem,
                     c->d_deltas, c->d_dists, c->d_rings, c->d_spill, c->d_counters, c->d_sf,
                     c->d_sb, c->d_tab_deltas, c->d_tab_dists, c->d_installed,
-                    c->d_rc_blocks, c->d_rc_offsets, c->d_rc_ids, c->d_bmax};
+                    c->d_rc_blocks, c->d_rc_offsets, c->d_rc_ids, c->d_bmax, c->d_qdem_rings,
+                    c->d_diag};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    drop_tvs_graph(c);
+    for (cudaEvent_t ev : {c->ev_begin, c->ev_shaped, c->ev_swept})
+        if (ev) cudaEventDestroy(ev);
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -186,6 +202,7 @@ tvs::SweepArgs sweep_args(tvs_context *c, uint32_t first, uint32_t count) {
     a.total = c->d_total;
     a.cumulative64 = c->d_cum64;
     a.reserved = c->g.reserved_rings_per_band;
+    a.ref_reserved = c->g.reserved_rings_per_band;
     a.half_bands = c->g.computable_points_count;
     return a;
 }
@@ -232,19 +249,35 @@ SweepImpl sweep_impl() {
     return v;
 }
 
-int ensure_rings(tvs_context *c) {
-    if (c->d_rings) return TVS_OK;
-    if (c->g.ring_slots_per_sector == 0)
+// Device ring buffer of `slots` u32 per band (the reference's reservation for
+// its layout, kCompactSlots for the compact stream), the spill list and the
+// counters; grown when a later call needs more slots.
+int ensure_rings(tvs_context *c, uint32_t slots) {
+    if (slots == 0)
         return fail(c, TVS_ERR_RING_OVERFLOW,
                     "no ring slots are reserved (rings_per_km * line of sight < 1 slot): the "
                     "reference's first ring write is out of bounds (kernel.rs:307)");
-    c->spill_cap = kSpillCap;
-    cudaError_t e = cudaMalloc(&c->d_rings, c->g.ring_slots_per_sector * sizeof(uint32_t));
-    if (e == cudaSuccess) e = cudaMalloc(&c->d_spill, (size_t)c->spill_cap * sizeof(uint4));
-    if (e == cudaSuccess) e = cudaMalloc(&c->d_counters, 4 * sizeof(uint32_t));
-    if (e == cudaSuccess)
-        c->device_bytes += c->g.ring_slots_per_sector * sizeof(uint32_t) +
-                           (size_t)c->spill_cap * sizeof(uint4) + 4 * sizeof(uint32_t);
+    const uint64_t need = c->g.total_bands * (uint64_t)slots;
+    cudaError_t e = cudaSuccess;
+    if (need > c->ring_capacity) {
+        if (c->d_rings) {
+            cudaFree(c->d_rings);
+            c->device_bytes -= c->ring_capacity * sizeof(uint32_t);
+            c->d_rings = nullptr;
+            c->ring_capacity = 0;
+        }
+        e = cudaMalloc(&c->d_rings, std::max<uint64_t>(need, 1) * sizeof(uint32_t));
+        if (e == cudaSuccess) {
+            c->ring_capacity = std::max<uint64_t>(need, 1);
+            c->device_bytes += c->ring_capacity * sizeof(uint32_t);
+        }
+    }
+    if (e == cudaSuccess && !c->d_spill) {
+        c->spill_cap = kSpillCap;
+        e = cudaMalloc(&c->d_spill, (size_t)c->spill_cap * sizeof(uint4));
+        if (e == cudaSuccess) e = cudaMalloc(&c->d_counters, 4 * sizeof(uint32_t));
+        if (e == cudaSuccess) c->device_bytes += (size_t)c->spill_cap * sizeof(uint4) + 4 * sizeof(uint32_t);
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
         return fail(c, e == cudaErrorMemoryAllocation ? TVS_ERR_OUT_OF_MEMORY : TVS_ERR_CUDA,
@@ -316,8 +349,40 @@ int upload_queue_dem(tvs_context *c) {
     return TVS_OK;
 }
 
-// Sweep sectors [first, first+count) (slots == angles).  With rings, count is 1.
-int enqueue_sweep(tvs_context *c, uint32_t first, uint32_t count, bool rings) {
+// The queue descriptor of this context tiled for the ring sweep's split
+// layout: the context's own when its configuration is a split layout, else
+// one for the precision's default split layout.
+int ring_queue_dem(tvs_context *c, const tvs::QueueDem **dem, uint32_t *tiles, int *layout) {
+    if (c->qcfg.layout != 0) {
+        int rc = upload_queue_dem(c);
+        if (rc) return rc;
+        *dem = c->d_qdem;
+        *tiles = c->q_tiles_per_sector;
+        *layout = c->qcfg.layout;
+        return TVS_OK;
+    }
+    const tvs::QueueConfig q = tvs::default_split_config((int)c->p.precision);
+    if (!c->d_qdem_rings) {
+        TVS_CUDA(c, cudaMalloc(&c->d_qdem_rings, sizeof(tvs::QueueDem)));
+        c->device_bytes += sizeof(tvs::QueueDem);
+        tvs::QueueDem d = queue_dem(c);
+        uint32_t done_total = 0;
+        tvs::queue_tile(&d, 1, q, &c->q_ring_tiles, &done_total);
+        TVS_CUDA(c, cudaMemcpy(c->d_qdem_rings, &d, sizeof d, cudaMemcpyHostToDevice));
+        c->ring_layout = (uint32_t)q.layout;
+    }
+    *dem = c->d_qdem_rings;
+    *tiles = c->q_ring_tiles;
+    *layout = (int)c->ring_layout;
+    return TVS_OK;
+}
+
+// Sweep sectors [first, first+count) (slots == angles).  ring_slots != 0:
+// count is 1 and the sector's ring records go to d_rings with ring_slots u32
+// per band (the reference's reservation for its layout, kCompactSlots for the
+// compact stream).
+int enqueue_sweep(tvs_context *c, uint32_t first, uint32_t count, uint32_t ring_slots) {
+    const bool rings = ring_slots != 0;
     if (c->p.sweep_kernel == TVS_SWEEP_PLAIN) {
         int rc = ensure_plain_scratch(c);
         if (rc) return rc;
@@ -336,7 +401,7 @@ int enqueue_sweep(tvs_context *c, uint32_t first, uint32_t count, bool rings) {
             a.dists = c->d_dists + (uint64_t)s * c->g.band_deltas_size;
             a.sf = c->d_sf;
             a.sb = c->d_sb;
-            a.reserved = c->g.reserved_rings_per_band;
+            a.reserved = rings ? ring_slots : c->g.reserved_rings_per_band;
             a.half_bands = c->g.computable_points_count;
             if (rings) {
                 a.rings = c->d_rings;
@@ -356,6 +421,40 @@ int enqueue_sweep(tvs_context *c, uint32_t first, uint32_t count, bool rings) {
     const uint32_t n_steps =
         c->g.band_steps_filled + std::min(c->g.band_deltas_size - c->g.band_steps_filled, 2u);
     const SweepImpl impl = sweep_impl();
+    if (rings && c->p.precision != TVS_PRECISION_FP64 && impl == SweepImpl::Queue) {
+        // ring records from the direction-split sweep itself
+        const tvs::QueueDem *dem = nullptr;
+        uint32_t tiles = 0;
+        int layout = 0;
+        int rc = ring_queue_dem(c, &dem, &tiles, &layout);
+        if (rc) return rc;
+        tvs::QueueArgs q{};
+        q.dems = dem;
+        q.n_dems = 1;
+        q.first_sector = first;
+        q.n_sectors = count;
+        q.tiles_per_sector = tiles;
+        q.max_step_cap = c->step_cap;
+        q.queue = c->d_queue;
+        q.done = c->d_done;
+        q.done_total = tiles;
+        q.done_cap = c->done_cap;
+        q.error = c->d_error;
+        q.spin_limit = c->spin_limit;
+        q.held_tile = c->held_tile;
+        q.rechecks = c->d_rechecks;
+        q.diag = c->diag_on ? c->d_diag : nullptr;
+        q.rings = c->d_rings;
+        q.ring_reserved = ring_slots;
+        q.ref_reserved = c->g.reserved_rings_per_band;
+        q.half_bands = c->g.computable_points_count;
+        q.spill = c->d_spill;
+        q.spill_cap = c->spill_cap;
+        q.ring_counters = c->d_counters;
+        TVS_CUDA(c, tvs::launch_sweep_split(q, (int)c->p.precision, layout, c->stream));
+        c->launches++;
+        return TVS_OK;
+    }
     if (!rings && impl == SweepImpl::Queue) {
         int rc = upload_queue_dem(c);
         if (rc) return rc;
@@ -374,6 +473,7 @@ int enqueue_sweep(tvs_context *c, uint32_t first, uint32_t count, bool rings) {
         q.spin_limit = c->spin_limit;
         q.held_tile = c->held_tile;
         q.rechecks = c->d_rechecks;
+        q.diag = c->diag_on ? c->d_diag : nullptr;
         TVS_CUDA(c, tvs::launch_sweep_queue(q, (int)c->p.precision, c->qcfg, c->stream));
         c->launches++;
         return TVS_OK;
@@ -392,8 +492,11 @@ int enqueue_sweep(tvs_context *c, uint32_t first, uint32_t count, bool rings) {
         }
         return TVS_OK;
     }
+    if (c->p.precision == TVS_PRECISION_FP32)
+        return fail(c, TVS_ERR_INVALID_ARGUMENT, "the FP32 form runs on the persistent sweep only");
     tvs::SweepArgs a = sweep_args(c, first, count);
     if (rings) {
+        a.reserved = ring_slots;
         a.rings = c->d_rings;
         a.spill = c->d_spill;
         a.spill_cap = c->spill_cap;
@@ -484,6 +587,7 @@ int fail_of(tvs_context *c, int code, const std::string &msg) { return fail(c, c
 int enqueue_shape_of(tvs_context *c, uint32_t first, uint32_t count) {
     return enqueue_shape(c, first, count);
 }
+void drop_tvs_graph_of(tvs_context *c) { drop_tvs_graph(c); }
 }  // namespace tvs_host
 
 extern "C" {
@@ -512,7 +616,7 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
     if (rc) return fail(nullptr, rc, msg);
     if (!elevations || n_elevations != g.size)
         return fail(nullptr, TVS_ERR_INVALID_ARGUMENT, "elevations must hold width*height values");
-    if (params->precision > TVS_PRECISION_FP64 || params->sweep_kernel > TVS_SWEEP_PLAIN ||
+    if (params->precision > TVS_PRECISION_FP32 || params->sweep_kernel > TVS_SWEEP_PLAIN ||
         (params->sweep_kernel == TVS_SWEEP_PLAIN && params->precision != TVS_PRECISION_EXACT32))
         return fail(nullptr, TVS_ERR_INVALID_ARGUMENT, "unsupported precision/sweep-kernel pair");
     uint32_t rb = params->tvs_row_begin, re = params->tvs_row_end;
@@ -572,6 +676,7 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
         {(void **)&c->d_hmax, sizeof(float)},
         {(void **)&c->d_bmax, (size_t)std::max<uint64_t>((uint64_t)c->bmax_w * c->bmax_h, 1) * sizeof(float)},
         {(void **)&c->d_rechecks, sizeof(unsigned long long)},
+        {(void **)&c->d_diag, 4 * sizeof(unsigned long long)},
         {(void **)&c->d_qdem, sizeof(tvs::QueueDem)},
         {(void **)&c->d_deltas, (size_t)slots * bds * sizeof(int32_t)},
         {(void **)&c->d_dists, (size_t)slots * bds * sizeof(float)},
@@ -580,7 +685,7 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
         if ((e = cudaMalloc(a.p, a.bytes)) != cudaSuccess) return bail(e, "cudaMalloc");
         c->device_bytes += a.bytes;
     }
-    if (params->precision != TVS_PRECISION_EXACT32) {
+    if (params->precision == TVS_PRECISION_MIXED64 || params->precision == TVS_PRECISION_FP64) {
         if ((e = cudaMalloc(&c->d_cum64, count * sizeof(double))) != cudaSuccess)
             return bail(e, "cudaMalloc");
         c->device_bytes += count * sizeof(double);
@@ -613,6 +718,7 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
     if ((e = cudaMemset(c->d_hdr, 0, slots * sizeof(tvs::ShapeHeader))) != cudaSuccess ||
         (e = cudaMemset(c->d_error, 0, sizeof(int32_t))) != cudaSuccess ||
         (e = cudaMemset(c->d_rechecks, 0, sizeof(unsigned long long))) != cudaSuccess ||
+        (e = cudaMemset(c->d_diag, 0, 4 * sizeof(unsigned long long))) != cudaSuccess ||
         (e = cudaMemset(c->d_cum, 0, count * sizeof(float))) != cudaSuccess ||
         (e = cudaMemset(c->d_total, 0, count * sizeof(float))) != cudaSuccess)
         return bail(e, "cudaMemset");
@@ -740,8 +846,9 @@ int tvs_compute_sector(tvs_context *ctx, uint32_t angle, float *cumulative_surfa
     // FP64/MIXED64 accumulate in double within the sector, from the caller's f32
     if (ctx->d_cum64 && count)
         TVS_CUDA(ctx, tvs::launch_widen(ctx->d_cum, ctx->d_cum64, count, ctx->stream));
+    const uint32_t R = ctx->g.reserved_rings_per_band;
     if (rings) {
-        int rc = ensure_rings(ctx);
+        int rc = ensure_rings(ctx, R);
         if (rc) return rc;
         TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_rings, 0,
                                       ctx->g.ring_slots_per_sector * sizeof(uint32_t), ctx->stream));
@@ -751,7 +858,7 @@ int tvs_compute_sector(tvs_context *ctx, uint32_t angle, float *cumulative_surfa
     if (rc) return rc;
     rc = header_status(ctx, angle, 1);
     if (rc) return rc;
-    rc = enqueue_sweep(ctx, angle, 1, rings != nullptr);
+    rc = enqueue_sweep(ctx, angle, 1, rings ? R : 0);
     if (rc) return rc;
     if (count)
         TVS_CUDA(ctx, cudaMemcpyAsync(cumulative_surfaces, ctx->d_cum, count * sizeof(float),
@@ -781,24 +888,30 @@ int tvs_compute_sector_rings(tvs_context *ctx, uint32_t angle, float *cumulative
                                       cudaMemcpyHostToDevice, ctx->stream));
     if (ctx->d_cum64 && count)
         TVS_CUDA(ctx, tvs::launch_widen(ctx->d_cum, ctx->d_cum64, count, ctx->stream));
-    int rc = ensure_rings(ctx);
+    int rc = ensure_rings(ctx, kCompactSlots);
     if (rc) return rc;
     const uint64_t bands = ctx->g.total_bands;
-    const uint32_t R = ctx->g.reserved_rings_per_band;
+    const uint32_t R = kCompactSlots;
     const uint64_t nb = tvs::ring_scan_blocks(bands);
     if (!ctx->d_rc_offsets) {
         TVS_CUDA(ctx, cudaMalloc(&ctx->d_rc_offsets, (bands + 1) * sizeof(uint64_t)));
         TVS_CUDA(ctx, cudaMalloc(&ctx->d_rc_blocks, (nb + 1) * sizeof(uint64_t)));
         ctx->device_bytes += (bands + 1 + nb + 1) * sizeof(uint64_t);
     }
-    TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_rings, 0, ctx->g.ring_slots_per_sector * sizeof(uint32_t),
-                                  ctx->stream));
+    // Every band the split sweep covers writes its count (slot 0) and its
+    // ids; the slots past a band's count are never read.  A row shard leaves
+    // the other bands unwritten (their counts must read 0), and the other
+    // sweeps write only where they have ids.
+    if (ctx->row_begin != 0 || ctx->row_end != ctx->g.tvs_height ||
+        ctx->p.sweep_kernel == TVS_SWEEP_PLAIN || ctx->p.precision == TVS_PRECISION_FP64 ||
+        sweep_impl() != SweepImpl::Queue)
+        TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_rings, 0, bands * R * sizeof(uint32_t), ctx->stream));
     TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), ctx->stream));
     rc = enqueue_shape(ctx, angle, 1);
     if (rc) return rc;
     rc = header_status(ctx, angle, 1);
     if (rc) return rc;
-    rc = enqueue_sweep(ctx, angle, 1, true);
+    rc = enqueue_sweep(ctx, angle, 1, R);
     if (rc) return rc;
     if (count)
         TVS_CUDA(ctx, cudaMemcpyAsync(cumulative_surfaces, ctx->d_cum, count * sizeof(float),
@@ -891,7 +1004,7 @@ int tvs_device_sweep_sectors(tvs_context *ctx, uint32_t first_angle, uint32_t co
             return fail(ctx, TVS_ERR_INVALID_ARGUMENT,
                         "sweep of a sector whose shape stage has not run");
     TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
-    return enqueue_sweep(ctx, first_angle, count, false);
+    return enqueue_sweep(ctx, first_angle, count, 0);
 }
 
 int tvs_device_run_sectors(tvs_context *ctx, uint32_t first_angle, uint32_t count) {
@@ -949,6 +1062,11 @@ int tvs_set_sweep_config(tvs_context *ctx, const tvs_sweep_config *cfg) {
         return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "unsupported points-per-thread shape");
     if (c.layout != 0 && ctx->p.precision == TVS_PRECISION_FP64)
         return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "sweep layouts 1-6 are not available for FP64");
+    if (c.layout == 0 && ctx->p.precision == TVS_PRECISION_FP32)
+        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "the FP32 form runs on sweep layouts 1-6 only");
+    if (c.px != ctx->qcfg.px || c.py != ctx->qcfg.py || c.packed != ctx->qcfg.packed ||
+        c.prefetch != ctx->qcfg.prefetch || c.layout != ctx->qcfg.layout)
+        drop_tvs_graph(ctx);
     ctx->qcfg = c;
     return TVS_OK;
 }
@@ -970,6 +1088,7 @@ int tvs_autotune(tvs_context *ctx, uint32_t sample_sectors, tvs_sweep_config *ch
     TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
     const bool exact = ctx->p.precision == TVS_PRECISION_EXACT32;
     const bool f64 = ctx->p.precision == TVS_PRECISION_FP64;
+    const bool fp32 = ctx->p.precision == TVS_PRECISION_FP32;
     const tvs::QueueConfig cands[] = {{1, 1, 0, 0, 0}, {2, 1, 0, 0, 0}, {4, 1, 0, 0, 0},
                                       {2, 2, 0, 0, 0}, {2, 1, 1, 0, 0}, {4, 1, 1, 0, 0},
                                       {1, 1, 0, 1, 0}, {2, 1, 0, 1, 0}, {4, 1, 0, 1, 0},
@@ -984,12 +1103,12 @@ int tvs_autotune(tvs_context *ctx, uint32_t sample_sectors, tvs_sweep_config *ch
     int rc = enqueue_shape(ctx, 0, sample_sectors);
     for (const tvs::QueueConfig &c : cands) {
         if (rc) break;
-        if ((c.packed && !exact) || (c.layout != 0 && f64)) continue;
+        if ((c.packed && !exact) || (c.layout != 0 && f64) || (c.layout == 0 && fp32)) continue;
         ctx->qcfg = c;
         float ms = 0.0f;
         for (int rep = 0; rep < 2 && rc == TVS_OK; rep++) {  // the first run warms up
             cudaEventRecord(t0, ctx->stream);
-            rc = enqueue_sweep(ctx, 0, sample_sectors, false);
+            rc = enqueue_sweep(ctx, 0, sample_sectors, 0);
             cudaEventRecord(t1, ctx->stream);
             if (rc == TVS_OK && cudaEventSynchronize(t1) != cudaSuccess)
                 rc = fail(ctx, TVS_ERR_CUDA, "autotune run failed");
@@ -1003,6 +1122,7 @@ int tvs_autotune(tvs_context *ctx, uint32_t sample_sectors, tvs_sweep_config *ch
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     ctx->qcfg = best_cfg;
+    drop_tvs_graph(ctx);
     for (bool &p : ctx->pending) p = false;
     if (rc) return rc;
     if (chosen) tvs_get_sweep_config(ctx, chosen);
@@ -1013,6 +1133,113 @@ int tvs_set_queue_wait(tvs_context *ctx, uint32_t spin_limit, uint32_t held_tile
     if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
     ctx->spin_limit = spin_limit ? spin_limit : tvs::kDefaultSpinLimit;
     ctx->held_tile = held_tile;
+    drop_tvs_graph(ctx);
+    return TVS_OK;
+}
+
+int tvs_set_sweep_counters(tvs_context *ctx, int enable) {
+    if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
+    TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
+    TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_diag, 0, 4 * sizeof(unsigned long long), ctx->stream));
+    if ((enable != 0) != ctx->diag_on) drop_tvs_graph(ctx);
+    ctx->diag_on = enable != 0;
+    return TVS_OK;
+}
+
+int tvs_read_sweep_counters(tvs_context *ctx, uint64_t *counters) {
+    if (!ctx || !counters) return TVS_ERR_INVALID_ARGUMENT;
+    TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
+    unsigned long long v[4];
+    TVS_CUDA(ctx, cudaMemcpyAsync(v, ctx->d_diag, sizeof v, cudaMemcpyDeviceToHost, ctx->stream));
+    TVS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int i = 0; i < 4; i++) counters[i] = v[i];
+    return TVS_OK;
+}
+
+int tvs_device_run_tvs(tvs_context *ctx) {
+    if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
+    TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
+    // reset, the 180 shape stages and the sweep, with the stage events
+    // (captured, the events become event-record nodes of the graph)
+    auto enqueue_tvs = [&](bool captured) -> int {
+        auto record = [&](cudaEvent_t ev) {
+            return captured ? cudaEventRecordWithFlags(ev, ctx->stream, cudaEventRecordExternal)
+                            : cudaEventRecord(ev, ctx->stream);
+        };
+        TVS_CUDA(ctx, record(ctx->ev_begin));
+        int rc = tvs_device_reset(ctx);
+        if (rc == TVS_OK) rc = enqueue_shape(ctx, 0, tvs::kSectorSteps);
+        if (rc) return rc;
+        TVS_CUDA(ctx, record(ctx->ev_shaped));
+        rc = enqueue_sweep(ctx, 0, tvs::kSectorSteps, 0);
+        if (rc) return rc;
+        TVS_CUDA(ctx, record(ctx->ev_swept));
+        return TVS_OK;
+    };
+    if (!ctx->tvs_exec) {
+        // The first call runs the sequence with plain launches (which loads the
+        // kernels and sets their launch attributes outside any capture), then
+        // captures the same sequence for the later calls.
+        for (cudaEvent_t *ev : {&ctx->ev_begin, &ctx->ev_shaped, &ctx->ev_swept})
+            if (!*ev) TVS_CUDA(ctx, cudaEventCreate(ev));
+        if (ctx->p.sweep_kernel == TVS_SWEEP_PLAIN) {
+            int rc = ensure_plain_scratch(ctx);
+            if (rc) return rc;
+        }
+        ctx->launches = 0;
+        int rc = enqueue_tvs(false);
+        for (uint32_t s = 0; s < tvs::kSectorSteps; s++) ctx->pending[s] = true;
+        if (rc) return rc;
+        const uint64_t plain = ctx->launches;
+        TVS_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        rc = enqueue_tvs(true);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+        if (rc != TVS_OK) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return rc;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&ctx->tvs_exec, g, 0);
+        if (e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            ctx->tvs_exec = nullptr;
+            cudaGetLastError();
+            return cuda_fail(ctx, e, "capturing the total-viewshed graph");
+        }
+        ctx->tvs_graph = g;
+        ctx->tvs_graph_launches = ctx->launches - plain;
+        ctx->launches = plain;
+        return TVS_OK;
+    }
+    TVS_CUDA(ctx, cudaGraphLaunch(ctx->tvs_exec, ctx->stream));
+    for (uint32_t s = 0; s < tvs::kSectorSteps; s++) ctx->pending[s] = true;
+    ctx->launches = ctx->tvs_graph_launches;
+    return TVS_OK;
+}
+
+int tvs_last_run_times(tvs_context *ctx, float *shape_ms, float *sweep_ms) {
+    if (!ctx || !ctx->ev_begin) return TVS_ERR_INVALID_ARGUMENT;
+    TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
+    TVS_CUDA(ctx, cudaEventSynchronize(ctx->ev_swept));
+    float a = 0.0f, b = 0.0f;
+    TVS_CUDA(ctx, cudaEventElapsedTime(&a, ctx->ev_begin, ctx->ev_shaped));
+    TVS_CUDA(ctx, cudaEventElapsedTime(&b, ctx->ev_shaped, ctx->ev_swept));
+    if (shape_ms) *shape_ms = a;
+    if (sweep_ms) *sweep_ms = b;
+    return TVS_OK;
+}
+
+int tvs_measure_l1_load(int32_t device, double *bytes_per_second) {
+    if (!bytes_per_second) return fail(nullptr, TVS_ERR_INVALID_ARGUMENT, "null argument");
+    cudaError_t e = cudaSetDevice(device);
+    double v = 0.0;
+    if (e == cudaSuccess) e = tvs::measure_l1_load(&v);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(nullptr, TVS_ERR_CUDA, std::string("l1 load: ") + cudaGetErrorString(e));
+    }
+    *bytes_per_second = v;
     return TVS_OK;
 }
 
@@ -1039,7 +1266,7 @@ int tvs_run(tvs_context *ctx, float *cumulative_out, float *total_out, int want_
     int rc = tvs_device_reset(ctx);
     if (rc) return rc;
     if (!want_rings) {
-        rc = tvs_device_run_sectors(ctx, 0, tvs::kSectorSteps);
+        rc = tvs_device_run_tvs(ctx);
         if (rc) return rc;
         rc = tvs_device_finish(ctx);
         if (rc) return rc;
@@ -1052,9 +1279,10 @@ int tvs_run(tvs_context *ctx, float *cumulative_out, float *total_out, int want_
             }
         return tvs_read_surfaces(ctx, cumulative_out, total_out);
     }
-    if (ctx->p.precision != TVS_PRECISION_EXACT32 && !ctx->d_cum64)
+    if ((ctx->p.precision == TVS_PRECISION_MIXED64 || ctx->p.precision == TVS_PRECISION_FP64) &&
+        !ctx->d_cum64)
         return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "FP64 context without FP64 accumulator");
-    rc = ensure_rings(ctx);
+    rc = ensure_rings(ctx, ctx->g.reserved_rings_per_band);
     if (rc) return rc;
     std::vector<uint32_t> host_rings(ctx->g.ring_slots_per_sector);
     for (uint32_t s = 0; s < tvs::kSectorSteps; s++) {
@@ -1065,7 +1293,7 @@ int tvs_run(tvs_context *ctx, float *cumulative_out, float *total_out, int want_
         if (rc) return rc;
         rc = header_status(ctx, s, 1);
         if (rc) return rc;
-        rc = enqueue_sweep(ctx, s, 1, true);
+        rc = enqueue_sweep(ctx, s, 1, ctx->g.reserved_rings_per_band);
         if (rc) return rc;
         tvs_sector_stats st{};
         st.angle = s;

@@ -147,6 +147,7 @@ int tvs_set_band_shape(tvs_context *ctx, uint32_t angle, const int32_t *band_del
     TVS_CCUDA(ctx, cudaMemcpyAsync(ctx->d_installed + angle, &one, 1, cudaMemcpyHostToDevice,
                                    ctx->stream));
     TVS_CCUDA(ctx, cudaStreamSynchronize(ctx->stream));  // the host tables may go away
+    if (!ctx->installed[angle]) tvs_host::drop_tvs_graph_of(ctx);  // one more shape launch
     ctx->installed[angle] = true;
     return TVS_OK;
 }
@@ -154,6 +155,7 @@ int tvs_set_band_shape(tvs_context *ctx, uint32_t angle, const int32_t *band_del
 int tvs_clear_band_shapes(tvs_context *ctx) {
     if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
     for (bool &b : ctx->installed) b = false;
+    tvs_host::drop_tvs_graph_of(ctx);
     if (!ctx->d_installed) return TVS_OK;
     TVS_CCUDA(ctx, cudaSetDevice(ctx->p.device));
     TVS_CCUDA(ctx, cudaMemsetAsync(ctx->d_installed, 0, tvs::kSectorSteps, ctx->stream));

@@ -73,7 +73,7 @@ __device__ __forceinline__ void ring_store(const SweepArgs &a, uint64_t kid, uin
 
 __device__ __forceinline__ void ring_finish(const SweepArgs &a, uint64_t kid, uint32_t n) {
     ring_store(a, kid, 0, n);
-    if (n >= a.reserved) atomicAdd(&a.counters[1], 1u);
+    if (n >= (a.ref_reserved ? a.ref_reserved : a.reserved)) atomicAdd(&a.counters[1], 1u);
     atomicMax(&a.counters[2], n);
 }
 
@@ -464,6 +464,26 @@ __global__ void __launch_bounds__(256) k_ffma_issue(float *out, int iters, float
     if (s == 1234.5f) out[0] = s;  // keeps the chains live
 }
 
+// L1 load-throughput probe: every warp reads 32 consecutive floats per load
+// (one 128-byte request, the sweep's access) from a 16 KB block-private
+// window that stays in L1, eight independent loads in flight per thread.
+__global__ void __launch_bounds__(256) k_l1_load(const float *src, float *out, int iters) {
+    const float *w = src + (size_t)blockIdx.x * 4096;
+    float acc[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[j] = 0.0f;
+    uint32_t o = threadIdx.x;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[j] = __fadd_rn(acc[j], __ldg(w + ((o + j * 512u) & 4095u)));
+        o = (o + 256u) & 4095u;
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 8; j++) s = __fadd_rn(s, acc[j]);
+    if (s == 1234.5f) out[0] = s;  // keeps the loads live
+}
+
 // out[0] = max |x| + |add| (non-negative floats order as their bit patterns).
 __global__ void k_max_abs(const float *x, uint64_t n, float add, unsigned int *out) {
     float m = 0.0f;
@@ -539,6 +559,38 @@ cudaError_t measure_fp32_issue(double *instructions_per_second) {
         *instructions_per_second = (double)blocks * 256.0 * iters * 8.0 / (best * 1e-3);
     if (t0) cudaEventDestroy(t0);
     if (t1) cudaEventDestroy(t1);
+    if (out) cudaFree(out);
+    return e;
+}
+
+cudaError_t measure_l1_load(double *bytes_per_second) {
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned blocks = (unsigned)sms * 4u;
+    float *src = nullptr, *out = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&src, (size_t)blocks * 4096 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(src, 0, (size_t)blocks * 4096 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&out, sizeof(float));
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreate(&t0);
+    if (e == cudaSuccess) e = cudaEventCreate(&t1);
+    const int iters = 1 << 13;
+    float best = 1e30f;
+    for (int rep = 0; rep < 4 && e == cudaSuccess; rep++) {
+        cudaEventRecord(t0);
+        k_l1_load<<<blocks, 256>>>(src, out, iters);
+        cudaEventRecord(t1);
+        e = cudaEventSynchronize(t1);
+        float ms = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, t0, t1);
+        if (rep > 0 && ms < best) best = ms;  // the first launch warms up
+    }
+    if (e == cudaSuccess)
+        *bytes_per_second = (double)blocks * 256.0 * iters * 8.0 * sizeof(float) / (best * 1e-3);
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+    if (src) cudaFree(src);
     if (out) cudaFree(out);
     return e;
 }

@@ -1,4 +1,6 @@
-// sweep_queue.cu -- persistent band-of-sight sweep over a (sector, tile) work queue.
+// sweep_queue.cu -- persistent band-of-sight sweep over a (sector, tile) work
+// queue: the row layouts, and the layout configuration shared with the
+// direction-split sweep.
 //
 // The arithmetic is the reference kernel's (kernel.rs:153-254), as in sweep.cu;
 // this file changes how the work is scheduled so that no wave of CTAs runs
@@ -21,10 +23,8 @@
 //    the table operands); forward and backward bands of a point of view run
 //    in the same loop; cum = (cum + forward) + backward keeps the reference's
 //    order.  Every step is evaluated.
-//  * Direction-split layouts (sweep_tile_split): a lane sweeps four points of
-//    view one direction at a time behind a warp-level filter (the exact
-//    arithmetic runs only where some chain may change state) and skips
-//    32-step segments that the DEM's block maxima rule out.
+//  * Direction-split layouts 1-6 live in sweep_split.cu; launch_sweep_queue
+//    dispatches to them.
 //  * Steps [0, n_fast) use the table division (Markstein, see sweep.cu); the
 //    zero-distance tail uses IEEE division.
 //
@@ -42,13 +42,16 @@
 
 #include "tvs.h"
 #include "tvs_internal.cuh"
+#include "queue_sched.cuh"
 
 namespace tvs {
 namespace {
 
-constexpr int kTileX = 32;
-constexpr int kTileY = 8;
-constexpr int kThreads = kTileX * kTileY;
+constexpr int kTileX = kQueueTileX;
+constexpr int kTileY = kQueueTileY;
+constexpr int kThreads = kQueueThreads;
+// the row layouts' tables start 16-byte aligned after the queue control block
+__host__ __device__ constexpr size_t row_ctl_bytes() { return (sizeof(QueueCtl) + 15) & ~(size_t)15; }
 
 __device__ __forceinline__ float div_table32(float e, float y, float d) {
     const float q = __fmul_rn(e, y);
@@ -96,37 +99,9 @@ __device__ __forceinline__ float gt01(float a, float b) {
     return r;
 }
 
-// Segments of the direction-split fast loop: kSegSteps steps whose samples are
-// bounded together.  Per segment: the range of the forward DEM offsets (x, y)
-// over its steps, the largest and smallest 1/d and the largest filter offset.
-#ifndef TVS_SEG_STEPS
-#define TVS_SEG_STEPS 32
-#endif
-constexpr uint32_t kSegSteps = TVS_SEG_STEPS;
-static_assert(kSegSteps >= 1 && kSegSteps <= 32,
-              "the staging reduces one segment per warp, one step per lane");
-struct __align__(16) SegBound {
-    int dx0, dx1, dy0, dy1;
-    float ymax, ymin, zmax, pad;
-};
-
 // One packed table entry: {y, y}, {-d, -d}, {d/R, d/R}, {d*tan1, d*tan1}.
 struct PackedStep {
     f32x2 y, nd, c, w;
-};
-
-struct QueueCtl {
-    QueueDem dem;           // the current item's DEM (copied from the descriptor array)
-    uint32_t item;
-    uint32_t dem_index;     // descriptor index of `dem`
-    uint32_t sector;        // the staged sector
-    uint32_t tile;          // the current item's tile within its DEM
-    int32_t sector_status;  // the staged sector's shape status
-    int32_t wait_status;    // this item's dependency wait
-    uint32_t n_steps;
-    uint32_t n_fast;
-    bool restage;
-    float hmax;             // the staged DEM's elevation range (estimate windows)
 };
 
 // Per-point state of one direction.
@@ -194,354 +169,34 @@ __device__ __forceinline__ void step_f64(Chain<kPrec> &c, float h, double hp, fl
 #ifndef TVS_MIX_MIN_BLOCKS
 #define TVS_MIX_MIN_BLOCKS 4
 #endif
-template <int kPrec, int kPx, int kPy, int kVar>
+template <int kPrec, int kPx, int kPy>
 constexpr int queue_min_blocks() {
-    return kVar >= 3                      ? TVS_MIX_MIN_BLOCKS
-           : kPrec != TVS_PRECISION_MIXED64 ? 1
+    return kPrec != TVS_PRECISION_MIXED64 ? 1
            : kPx * kPy <= 2               ? TVS_MIX_MIN_BLOCKS
            : kPx * kPy == 4               ? 2
                                           : 1;
 }
 
-// MIXED64 and exact f32, one direction at a time.  A warp holds LX columns x 32/LX rows of
-// lanes and each lane four points of view LX columns apart; the 8 warps of a
-// CTA stack in rows: a tile is 4 LX x 256/LX points (layout 1: LX = 8, 32 x 32;
-// layout 2: LX = 16, 64 x 16; layout 3: LX = 32, 128 x 8).  A lane sweeps its
-// four forward chains over all steps, then its four backward chains.  Chains
-// of one direction over a compact patch of points of view see their running
-// maximum rise at nearly the same steps, so a warp enters the classification
-// at fewer steps than when it mixes directions; narrower patches gain more
-// there and pay more L1 sectors per load (rows of LX * 4 bytes).
-constexpr int kSplitCols = 4;  // points of view per lane
-// Layouts 4-6 are layouts 1-3 with each lane's four points of view as 2 columns
-// (LX apart) x 2 rows (32/LX apart): patches twice as tall and half as wide.
-__host__ __device__ constexpr int split_lx(int layout) { return 4 << ((layout - 1) % 3 + 1); }
-__host__ __device__ constexpr int split_ky(int layout) { return layout > 3 ? 2 : 1; }
-__host__ __device__ constexpr int split_tile_w(int layout) {
-    return kSplitCols / split_ky(layout) * split_lx(layout);
-}
-__host__ __device__ constexpr int split_tile_h(int layout) {
-    return kTileY * (32 / split_lx(layout)) * split_ky(layout);
-}
-
-// unroll factors of the direction-split fast loops (exact f32: 2, the best of 1-4
-// on one B200; MIXED64: 1, which keeps its state within 64 registers)
-#ifndef TVS_SPLIT_UNROLL
-#define TVS_SPLIT_UNROLL 2
-#endif
-#ifndef TVS_SPLIT_UNROLL_MIX
-#define TVS_SPLIT_UNROLL_MIX 1
-#endif
-#define TVS_PRAGMA(x) _Pragma(#x)
-#define TVS_UNROLL(n) TVS_PRAGMA(unroll n)
-
-// The filter threshold of an exact-f32 chain: m - |m| 2^-19 (one rounding).
-__device__ __forceinline__ float exact_lo(float m) { return __fmaf_rn(fabsf(m), -0x1p-19f, m); }
-
-template <int kPrec, int LX, int KY, class Wait>
-__device__ __forceinline__ void sweep_tile_split(const QueueArgs &a, const QueueDem &D, uint32_t bx,
-                                                 uint32_t by, uint32_t n, uint32_t n_fast,
-                                                 const float4 *s_steps, const long long *s_boff,
-                                                 const double *s_c64, const float *s_zf,
-                                                 const SegBound *s_seg, const float &hmax,
-                                                 void *s_fwd_raw, Wait &&wait_prev) {
-    constexpr bool kMix = kPrec == TVS_PRECISION_MIXED64;
-    using S = typename std::conditional<kMix, double, float>::type;  // surfaces
-    constexpr int K = kSplitCols, KX = K / KY, LY = 32 / LX;
-    // chain k: column tx + LX (k % KX), row ty + LY (k / KX)
-    const uint32_t lx = threadIdx.x % LX, ly = threadIdx.x / LX;
-    const uint32_t tx = bx * (KX * LX) + lx;
-    const uint32_t ty = D.row_begin + by * (kTileY * LY * KY) + threadIdx.y * LY * KY + ly;
-    // rows past the grid are clamped, columns past it read padding; both are discarded
-    const float *ep[KY];
-#pragma unroll
-    for (int r = 0; r < KY; r++)
-        ep[r] = D.elev + (int64_t)(min(ty + LY * r, D.row_end - 1) + D.los) * D.width + tx + D.los;
-    float hp32[K];  // kernel.rs:134 (the exact-f32 observer elevation)
-#pragma unroll
-    for (int k = 0; k < K; k++) hp32[k] = __fadd_rn(__ldg(ep[k / KX] + LX * (k % KX)), D.observer_height);
-    auto hp64 = [&](int k) -> double {
-        return __dadd_rn((double)__ldg(ep[k / KX] + LX * (k % KX)), (double)D.observer_height);
-    };
-    // forward surfaces wait in shared memory (s_fwd[k * kThreads + tid]) while
-    // the backward chains run
-    S *s_fwd = reinterpret_cast<S *>(s_fwd_raw);
-    const uint32_t tid = threadIdx.y * kTileX + threadIdx.x;
-    S sb[K];
-    // one direction's sweep; DIR is a compile-time 0 (forward) or 1 (backward)
-    auto pass = [&](auto DIR) {
-        constexpr int dir = decltype(DIR)::value;
-        // the sample of chain k at a step whose byte offset is b
-        auto at = [&](uint32_t step, int k) -> const float * {
-            const long long b = s_boff[step];
-            return (const float *)((const char *)ep[k / KX] + (dir ? -b : b)) + LX * (k % KX);
-        };
-        // The largest elevation any lane of this warp samples in a segment: the
-        // block maxima over the warp's patch of points of view moved by the
-        // segment's offset range (warp-uniform).
-        auto segment_max = [&](const SegBound &b) -> float {
-            const int px0 = (int)(bx * (KX * LX) + D.los), px1 = px0 + KX * LX - 1;
-            const int py0 = (int)(D.row_begin + by * (kTileY * LY * KY) + threadIdx.y * LY * KY + D.los);
-            const int py1 = py0 + LY * KY - 1;
-            const int x0 = dir ? px0 - b.dx1 : px0 + b.dx0, x1 = dir ? px1 - b.dx0 : px1 + b.dx1;
-            const int y0 = dir ? py0 - b.dy1 : py0 + b.dy0, y1 = dir ? py1 - b.dy0 : py1 + b.dy1;
-            const int bx0 = max(x0, 0) / (int)kBlockMax;
-            const int bx1 = min(max(x1, 0) / (int)kBlockMax, (int)D.bmax_w - 1);
-            const int by0 = max(y0, 0) / (int)kBlockMax;
-            const int by1 = min(max(y1, 0) / (int)kBlockMax, (int)D.bmax_h - 1);
-            const int nx = bx1 - bx0 + 1, cells = nx > 0 && by1 >= by0 ? nx * (by1 - by0 + 1) : 0;
-            float m = -INFINITY;
-            for (int q = (int)threadIdx.x; q < cells; q += 32)
-                m = fmaxf(m, __ldg(D.bmax + (size_t)(by0 + q / nx) * D.bmax_w + bx0 + q % nx));
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-            return m;
-        };
-        // A segment can be skipped when no chain's filter can pass at any of its
-        // steps: with e <= RN(B - h_pov) for every sample, fma(e, y, z) at a step
-        // is at most fma(RN(B - h_pov), y_max or y_min, z_max) (RN and fma are
-        // monotone), so a bound below the chain's threshold rules the whole
-        // segment out exactly as the per-step filter would.
-        auto skippable = [&](uint32_t seg, auto &&lo_of) -> bool {
-            const SegBound b = s_seg[seg];
-            const float B = segment_max(b);
-            bool skip = true;
-#pragma unroll
-            for (int k = 0; k < K; k++) {
-                const float E = __fsub_rn(B, hp32[k]);
-                skip &= __fmaf_rn(E, E >= 0.0f ? b.ymax : b.ymin, b.zmax) < lo_of(k);
-            }
-            return __all_sync(0xffffffffu, skip);
-        };
-        S out[K];
-        uint32_t i = 0;
-        if constexpr (kMix) {
-            auto exact_angle = [&](int k, uint32_t step) -> double {
-                // the FP64 table values {1/d, d/R} of the shape stage (fp64_step)
-                const double ek = __dsub_rn((double)__ldg(at(step, k)), hp64(k));
-                const double dd = (double)s_steps[step].w;
-                return __dsub_rn(div_table64(ek, __drcp_rn(dd), dd), s_c64[step]);
-            };
-            auto max64 = [&](int k, int32_t j) -> double {
-                return j < 0 ? -2000.0 : exact_angle(k, (uint32_t)j);
-            };
-            Chain<TVS_PRECISION_MIXED64> c[K];
-            // the step of each chain's maximum lives in shared memory: it is
-            // written at every raise but read only on the rare re-decisions
-            int32_t *jk = reinterpret_cast<int32_t *>(reinterpret_cast<S *>(s_fwd_raw) + K * kThreads) + tid;
-#pragma unroll
-            for (int k = 0; k < K; k++) {
-                c[k].init();
-                jk[k * kThreads] = -1;
-            }
-            for (uint32_t seg = 0; i < n_fast; seg++) {
-            const uint32_t i1 = min(i + kSegSteps, n_fast);
-            if (skippable(seg, [&](int k) { return c[k].lo; })) {
-                i = i1;
-                continue;
-            }
-            TVS_UNROLL(TVS_SPLIT_UNROLL_MIX)
-            for (; i < i1; i++) {
-                const float4 t = s_steps[i];
-                // filter (see the row layout): estimate + g >= m32 - gm
-                float e[K];
-                bool hit = false;
-#pragma unroll
-                for (int k = 0; k < K; k++) {
-                    e[k] = __fsub_rn(__ldg(at(i, k)), hp32[k]);
-                    hit |= __fmaf_rn(e[k], t.x, t.y) >= c[k].lo;
-                }
-                if (!__any_sync(0xffffffffu, hit)) continue;
-                const double w64 = __dmul_rn((double)t.w, 0.0174533);  // fp64_step(d).z
-                // the estimate window of the staging, recomputed bit for bit
-                const float gw = __fadd_rn(__fmul_rn(0x1p-20f, __fsub_rn(__fmul_rn(hmax, t.x), t.z)),
-                                           0x1p-90f);
-                float ah[K], dd[K];
-                bool any_amb = false;
-#pragma unroll
-                for (int k = 0; k < K; k++) {
-                    ah[k] = __fmaf_rn(e[k], t.x, t.z);
-                    dd[k] = __fsub_rn(ah[k], c[k].m32);
-                    const bool am = fabsf(dd[k]) <= __fadd_rn(gw, c[k].gm);
-                    if (!am && dd[k] > 0.0f) {  // surely visible
-                        c[k].set_max32(ah[k], gw);
-                        jk[k * kThreads] = (int32_t)i;
-                        c[k].s = __dadd_rn(c[k].s, w64);
-                    }
-                    any_amb |= am;
-                }
-                if (__any_sync(0xffffffffu, any_amb)) {
-                    // a chain surely visible at this step has j == i; every other
-                    // chain still has the state it was tested with
-#pragma unroll
-                    for (int k = 0; k < K; k++) {
-                        const int32_t jm = jk[k * kThreads];
-                        if (jm == (int32_t)i) continue;
-                        if (!(fabsf(dd[k]) <= __fadd_rn(gw, c[k].gm))) continue;
-                        if (a.rechecks) atomicAdd(a.rechecks, 1ull);
-                        const double a64 = exact_angle(k, i);
-                        if (a64 > max64(k, jm)) {
-                            jk[k * kThreads] = (int32_t)i;
-                            c[k].set_max32(ah[k], gw);
-                            c[k].s = __dadd_rn(c[k].s, w64);
-                        }
-                    }
-                }
-            }
-            }
-#pragma unroll
-            for (int k = 0; k < K; k++) c[k].m = max64(k, jk[k * kThreads]);
-            // the steps past the table-division domain (zero distances), IEEE division
-            for (; i < n; i++) {
-                const float dist = s_steps[i].w;
-                const double dd = (double)dist;
-                const double4 dt = make_double4(__drcp_rn(dd), s_c64[i], __dmul_rn(dd, 0.0174533), dd);
-                const int slow = !(dist >= 0x1p-20f && dist <= 0x1p20f);
-#pragma unroll
-                for (int k = 0; k < K; k++)
-                    step_f64<TVS_PRECISION_MIXED64, false>(c[k], __ldg(at(i, k)), hp64(k), dist, dt,
-                                                           slow);
-            }
-#pragma unroll
-            for (int k = 0; k < K; k++) out[k] = c[k].s;
-        } else {
-            // Exact f32: the angle is computed exactly (kernel.rs:168-190) only at
-            // steps where some lane's estimate is not surely below its maximum:
-            // e y - d/R + g >= m - |m| 2^-19, where g >= 4 x 2^-22 (d/R + hmax/d)
-            // and |m| 2^-19 bound the estimate's distance from the exact angle
-            // with room for the test's own two roundings.  A skipped step has
-            // angle <= m (or NaN): not visible and no change of m, as in the
-            // reference.
-            Chain<TVS_PRECISION_EXACT32> c[K];
-            float lo[K];
-#pragma unroll
-            for (int k = 0; k < K; k++) {
-                c[k].init();
-                lo[k] = exact_lo(c[k].m);
-            }
-            for (uint32_t seg = 0; i < n_fast; seg++) {
-            const uint32_t i1 = min(i + kSegSteps, n_fast);
-            if (skippable(seg, [&](int k) { return lo[k]; })) {
-                i = i1;
-                continue;
-            }
-            TVS_UNROLL(TVS_SPLIT_UNROLL)
-            for (; i < i1; i++) {
-                const float4 t = s_steps[i];
-                const float zf = s_zf[i];
-                float e[K];
-                bool hit = false;
-#pragma unroll
-                for (int k = 0; k < K; k++) {
-                    e[k] = __fsub_rn(__ldg(at(i, k)), hp32[k]);  // kernel.rs:164
-                    hit |= __fmaf_rn(e[k], t.x, zf) >= lo[k];
-                }
-                if (!__any_sync(0xffffffffu, hit)) continue;
-#pragma unroll
-                for (int k = 0; k < K; k++) {
-                    const float ang = __fsub_rn(div_table32(e[k], t.x, t.y), t.z);
-                    if (ang > c[k].m) c[k].s = __fadd_rn(c[k].s, t.w);
-                    c[k].m = fmaxf(ang, c[k].m);  // f32::max: NaN yields the other operand
-                    lo[k] = exact_lo(c[k].m);
-                }
-            }
-            }
-            for (; i < n; i++) {
-                const float4 t = s_steps[i];
-                const int slow = !(t.y >= 0x1p-20f && t.y <= 0x1p20f);
-#pragma unroll
-                for (int k = 0; k < K; k++)
-                    step_f32<TVS_PRECISION_EXACT32, false>(c[k], __ldg(at(i, k)), hp32[k], t, slow);
-            }
-#pragma unroll
-            for (int k = 0; k < K; k++) out[k] = c[k].s;
-        }
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-            if (dir == 0) s_fwd[k * kThreads + tid] = out[k];
-            else sb[k] = out[k];
-        }
-    };
-    pass(std::integral_constant<int, 0>{});
-    pass(std::integral_constant<int, 1>{});
-    const bool write = wait_prev();  // every thread of the CTA reaches it
-    if (!write) return;
-#pragma unroll
-    for (int k = 0; k < K; k++) {
-        const uint32_t col = tx + LX * (k % KX), row = ty + LY * (k / KX);
-        if (col >= D.tvs_width || row >= D.row_end) continue;
-        const uint64_t p = (uint64_t)row * D.tvs_width + col;
-        // forward surface first (kernel.rs:254), in L2 like the row layout
-        if constexpr (kMix) {
-            const double cum =
-                __dadd_rn(__dadd_rn(__ldcg(D.cumulative64 + p), s_fwd[k * kThreads + tid]), sb[k]);
-            __stcg(D.cumulative64 + p, cum);
-            const float c32 = __double2float_rn(cum);
-            __stcg(D.cumulative + p, c32);
-            if (D.total) __stcg(D.total + p, __fadd_rn(__ldcg(D.total + p), c32));
-        } else {
-            const float cum =
-                __fadd_rn(__fadd_rn(__ldcg(D.cumulative + p), s_fwd[k * kThreads + tid]), sb[k]);
-            __stcg(D.cumulative + p, cum);
-            if (D.total) __stcg(D.total + p, __fadd_rn(__ldcg(D.total + p), cum));  // compute.rs:206-214
-        }
-    }
-}
-
-// kVar: 0 scalar, 1 packed f32x2 (exact f32 only), 2 scalar with the next
-// step's elevations loaded while the current step computes, 3-8 the
-// direction-split layouts 1-6 above (kPx, kPy unused).
+// Row layouts.  kVar: 0 scalar, 1 packed f32x2 (exact f32 only), 2 scalar with
+// the next step's elevations loaded while the current step computes.
 template <int kPrec, int kPx, int kPy, int kVar>
-__global__ void __launch_bounds__(kThreads, (queue_min_blocks<kPrec, kPx, kPy, kVar>()))
+__global__ void __launch_bounds__(kThreads, (queue_min_blocks<kPrec, kPx, kPy>()))
 k_sweep_queue(QueueArgs a) {
     constexpr bool kPacked = kVar == 1;
     constexpr bool kPipe = kVar == 2;
-    constexpr bool kSplit = kVar >= 3;
     constexpr bool kMix = kPrec == TVS_PRECISION_MIXED64;
-    static_assert(!kSplit || kPrec != TVS_PRECISION_FP64, "no direction-split layout for FP64");
     constexpr bool kF64 = kPrec == TVS_PRECISION_FP64 || kMix;  // FP64 tables and surfaces
     extern __shared__ __align__(16) unsigned char smem[];
     QueueCtl &ctl = *reinterpret_cast<QueueCtl *>(smem);
-    float4 *s_steps = reinterpret_cast<float4 *>(smem + sizeof(QueueCtl));
+    float4 *s_steps = reinterpret_cast<float4 *>(smem + row_ctl_bytes());
     // forward DEM-id offset of each step, in bytes (a 64-bit add per base address)
     long long *s_boff = reinterpret_cast<long long *>(s_steps + a.max_step_cap);
     double4 *s_dtab = reinterpret_cast<double4 *>(s_boff + a.max_step_cap);  // FP64 rows only
     PackedStep *s_pk = reinterpret_cast<PackedStep *>(s_boff + a.max_step_cap);  // packed only
-    // direction-split layouts: 8 B more per step (MIXED64: d/R in double;
-    // exact f32: the filter offset), then the forward surfaces
-    double *s_c64 = reinterpret_cast<double *>(s_boff + a.max_step_cap);
-    float *s_zf = reinterpret_cast<float *>(s_boff + a.max_step_cap);
-    SegBound *s_seg = reinterpret_cast<SegBound *>(s_c64 + a.max_step_cap);
-    void *s_fwd = s_seg + (a.max_step_cap + kSegSteps - 1) / kSegSteps;
     const uint32_t tid = threadIdx.y * kTileX + threadIdx.x;
-    const uint32_t n_items = a.tiles_per_sector * a.n_sectors;
-    if (tid == 0) {
-        ctl.dem_index = 0xFFFFFFFFu;
-        ctl.sector = 0xFFFFFFFFu;
-    }
+    queue_init(ctl, tid);
 
-    for (;;) {
-        if (tid == 0) {
-            const uint32_t item = atomicAdd(a.queue, 1u);
-            ctl.item = item;
-            if (item < n_items) {
-                const uint32_t s = item / a.tiles_per_sector;
-                const uint32_t r = item - s * a.tiles_per_sector;
-                // the DEM whose tiles hold r (tile_base ascends)
-                uint32_t lo = 0, hi = a.n_dems - 1;
-                while (lo < hi) {
-                    const uint32_t mid = (lo + hi + 1) >> 1;
-                    if (a.dems[mid].tile_base <= r) lo = mid; else hi = mid - 1;
-                }
-                ctl.restage = lo != ctl.dem_index || s != ctl.sector;
-                if (lo != ctl.dem_index) ctl.dem = a.dems[lo];
-                ctl.dem_index = lo;
-                ctl.sector = s;
-                ctl.tile = r - ctl.dem.tile_base;
-            }
-        }
-        __syncthreads();
-        if (ctl.item >= n_items) break;
+    while (queue_next(a, ctl, tid)) {
         const QueueDem &D = ctl.dem;
         const uint32_t s = ctl.sector, tile = ctl.tile;
         if (ctl.restage) {  // stage this DEM's sector tables
@@ -550,24 +205,9 @@ k_sweep_queue(QueueArgs a) {
             const uint32_t n = h->n_steps;
             const float4 *gs = D.steps + (uint64_t)slot * D.step_cap;
             const int2 *go = D.offs + (uint64_t)slot * D.step_cap;
-            const float hmax = (kMix || kSplit) ? *D.hmax : 0.0f;
+            const float hmax = kMix ? *D.hmax : 0.0f;
             for (uint32_t i = tid; i < n; i += kThreads) {
                 const float4 t = gs[i];
-                if constexpr (kSplit) {
-                    // the estimate window g as below
-                    const float g = __fadd_rn(__fmul_rn(0x1p-20f, __fadd_rn(t.z, __fmul_rn(hmax, t.x))),
-                                              0x1p-90f);
-                    s_boff[i] = (long long)go[i].x * (long long)sizeof(float);
-                    if constexpr (kMix) {
-                        // {1/d, filter offset, -d/R, d}: g is recomputed where needed
-                        s_steps[i] = make_float4(t.x, __fadd_rn(-t.z, g), -t.z, t.y);
-                        s_c64[i] = D.dtab[(uint64_t)slot * D.step_cap + i].y;
-                    } else {
-                        s_steps[i] = t;
-                        s_zf[i] = __fadd_rn(-t.z, g);
-                    }
-                    continue;
-                }
                 s_steps[i] = t;
                 if (kMix) {
                     // decision window of the FP32 estimate at this step: at least 4x
@@ -591,36 +231,6 @@ k_sweep_queue(QueueArgs a) {
                     s_pk[i] = p;
                 }
             }
-            if constexpr (kSplit) {
-                // segment bounds of the fast steps, one warp per segment
-                __syncthreads();
-                const uint32_t nf = h->n_fast, lane = threadIdx.x;
-                const long long W = D.width;
-                for (uint32_t sg = threadIdx.y; sg * kSegSteps < nf; sg += kTileY) {
-                    const uint32_t i = sg * kSegSteps + lane;
-                    const bool v = lane < kSegSteps && i < nf;
-                    // the step's forward offset as (x, y): |x| < W/2 on every band of sight
-                    const long long off = v ? s_boff[i] / (long long)sizeof(float) : 0;
-                    const long long q = off + W / 2;
-                    const long long dy = q >= 0 ? q / W : -((W - 1 - q) / W);
-                    const int dx = (int)(off - dy * W);
-                    int dx0 = v ? dx : INT_MAX, dx1 = v ? dx : INT_MIN;
-                    int dy0 = v ? (int)dy : INT_MAX, dy1 = v ? (int)dy : INT_MIN;
-                    float ymax = v ? s_steps[i].x : -INFINITY, ymin = v ? s_steps[i].x : INFINITY;
-                    float zmax = v ? (kMix ? s_steps[i].y : s_zf[i]) : -INFINITY;
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) {
-                        dx0 = min(dx0, __shfl_xor_sync(0xffffffffu, dx0, o));
-                        dx1 = max(dx1, __shfl_xor_sync(0xffffffffu, dx1, o));
-                        dy0 = min(dy0, __shfl_xor_sync(0xffffffffu, dy0, o));
-                        dy1 = max(dy1, __shfl_xor_sync(0xffffffffu, dy1, o));
-                        ymax = fmaxf(ymax, __shfl_xor_sync(0xffffffffu, ymax, o));
-                        ymin = fminf(ymin, __shfl_xor_sync(0xffffffffu, ymin, o));
-                        zmax = fmaxf(zmax, __shfl_xor_sync(0xffffffffu, zmax, o));
-                    }
-                    if (lane == 0) s_seg[sg] = SegBound{dx0, dx1, dy0, dy1, ymax, ymin, zmax, 0.0f};
-                }
-            }
             if (tid == 0) {
                 ctl.sector_status = h->status;
                 ctl.n_steps = n;
@@ -632,39 +242,13 @@ k_sweep_queue(QueueArgs a) {
         // The tile's previous sector must be complete before this sector's
         // surfaces are added (bounded wait).  It is awaited after the sweep,
         // by which time it has almost always finished.
-        auto wait_prev = [&]() -> bool {
-        if (tid == 0) {
-            ctl.wait_status = TVS_OK;
-            if (s > 0) {
-                const volatile uint32_t *d = a.done + D.done_base + tile;
-                const volatile int32_t *err = a.error;
-                uint32_t spins = 0;
-                while (*d < s) {
-                    // give up at the limit, or at once when another wait already did
-                    if (++spins > a.spin_limit || *err != 0) {
-                        atomicExch(a.error, (int32_t)TVS_ERR_TIMEOUT);
-                        ctl.wait_status = TVS_ERR_TIMEOUT;
-                        break;
-                    }
-                    __nanosleep(256);
-                }
-                __threadfence();
-            }
-        }
-        __syncthreads();
-        return ctl.wait_status == TVS_OK;
-        };
+        auto wait_prev = [&]() -> bool { return queue_wait_prev(a, ctl, D, s, tile, tid); };
         const bool run = ctl.sector_status == TVS_OK;
         const uint32_t n = ctl.n_steps, n_fast = ctl.n_fast;
         const uint32_t bx = tile % D.tiles_x, by = tile / D.tiles_x;
         const uint32_t tx0 = bx * (kTileX * kPx) + threadIdx.x;
         const uint32_t ty0 = D.row_begin + by * (kTileY * kPy) + threadIdx.y;
-        if constexpr (kSplit) {
-            if (run)
-                sweep_tile_split<kPrec, split_lx(kVar - 2), split_ky(kVar - 2)>(
-                    a, D, bx, by, n, n_fast, s_steps, s_boff, s_c64, s_zf, s_seg, ctl.hmax, s_fwd,
-                    wait_prev);
-        } else if (run) {
+        if (run) {
             const float *ep[kPy];
             using HP = typename std::conditional<kF64, double, float>::type;
             HP hp[kPy][kPx];
@@ -986,56 +570,14 @@ k_sweep_queue(QueueArgs a) {
                 }
             }
         }
-        __threadfence();   // this thread's surface writes before the tile's counter
-        __syncthreads();
-        if (tid == 0 && D.done_base + tile != a.held_tile) atomicAdd(a.done + D.done_base + tile, 1u);
+        queue_done(a, D, tile, tid);
     }
 }
 
 template <int kPrec, int kPx, int kPy, int kVar>
 cudaError_t launch_queue_t(const QueueArgs &a, size_t smem, cudaStream_t s) {
-    auto fn = k_sweep_queue<kPrec, kPx, kPy, kVar>;
-    // the shared-memory attribute and the occupancy, per device (they belong to
-    // the device current at launch).  Contexts on several devices or host
-    // threads may launch this kernel concurrently, so the attribute only grows:
-    // a launch never finds it below its own shared memory.
-    struct Occupancy {
-        size_t attr = 0, smem = 0;
-        int blocks = -1;
-    };
-    static std::mutex mu;
-    static Occupancy occ[64];
-    int dev = 0, sms = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    int blocks_per_sm;
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        Occupancy &o = occ[dev];
-        if (smem > o.attr) {
-            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-            o.attr = smem;
-        }
-        if (o.blocks < 0 || o.smem != smem) {
-            int b = 0;
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreads, smem);
-            if (e != cudaSuccess) return e;
-            o.blocks = b < 1 ? 1 : b;
-            o.smem = smem;
-        }
-        blocks_per_sm = o.blocks;
-    }
-    if (a.done_total > a.done_cap) return cudaErrorInvalidValue;
-    e = cudaMemsetAsync(a.queue, 0, sizeof(uint32_t), s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(a.done, 0, (size_t)a.done_total * sizeof(uint32_t), s);
-    if (e != cudaSuccess) return e;
-    const uint64_t items = (uint64_t)a.tiles_per_sector * a.n_sectors;
-    const uint32_t grid = (uint32_t)std::min<uint64_t>((uint64_t)blocks_per_sm * sms, items);
-    fn<<<grid, dim3(kTileX, kTileY), smem, s>>>(a);
-    return cudaGetLastError();
+    return launch_persistent(reinterpret_cast<const void *>(&k_sweep_queue<kPrec, kPx, kPy, kVar>),
+                             a, smem, s);
 }
 
 }  // namespace
@@ -1075,21 +617,26 @@ QueueConfig default_queue_config(int precision) {
         if (f) d.prefetch = atoi(f) != 0;
         return d;
     }();
-    // MIXED64 defaults to layout 1 and exact f32 to layout 4 (the fastest on
-    // one B200 at 3601^2); TVS_SWEEP_LAYOUT and TVS_SWEEP_LAYOUT32 override them
-    static const int split = [] {
-        const char *l = getenv("TVS_SWEEP_LAYOUT");
-        return l ? atoi(l) : 1;
-    }();
-    static const int split32 = [] {
-        const char *l = getenv("TVS_SWEEP_LAYOUT32");
-        return l ? atoi(l) : 4;
-    }();
-    const int l = precision == TVS_PRECISION_MIXED64 ? split
-                  : precision == TVS_PRECISION_EXACT32 ? split32
-                                                       : 0;
-    if (l >= 1 && l <= 6) return QueueConfig{kSplitCols, 1, 0, 0, l};
-    return v;
+    if (precision == TVS_PRECISION_FP64) return v;
+    return default_split_config(precision);
+}
+
+QueueConfig default_split_config(int precision) {
+    // the fastest split layout per precision on one B200 at 3601^2;
+    // TVS_SWEEP_LAYOUT (MIXED64), TVS_SWEEP_LAYOUT32 (exact f32) and
+    // TVS_SWEEP_LAYOUT_FP32 override them
+    auto env_layout = [](const char *name, int d) {
+        const char *l = getenv(name);
+        const int v = l ? atoi(l) : d;
+        return v >= 1 && v <= 6 ? v : d;
+    };
+    static const int mix = env_layout("TVS_SWEEP_LAYOUT", 1);
+    static const int exact = env_layout("TVS_SWEEP_LAYOUT32", 4);
+    static const int fp32 = env_layout("TVS_SWEEP_LAYOUT_FP32", 4);
+    const int l = precision == TVS_PRECISION_MIXED64 ? mix
+                  : precision == TVS_PRECISION_FP32  ? fp32
+                                                     : exact;
+    return QueueConfig{kSplitCols, 1, 0, 0, l};
 }
 
 void queue_tile(QueueDem *dems, uint32_t n_dems, const QueueConfig &c, uint32_t *tiles_per_sector,
@@ -1113,24 +660,22 @@ void queue_tile(QueueDem *dems, uint32_t n_dems, const QueueConfig &c, uint32_t 
 cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, const QueueConfig &c,
                                cudaStream_t s) {
     if (a.n_dems == 0 || a.tiles_per_sector == 0 || a.n_sectors == 0) return cudaSuccess;
+    if (!queue_config_valid(c)) return cudaErrorInvalidValue;
+    if (c.layout != 0) {  // direction-split layouts (sweep_split.cu)
+        if (precision == TVS_PRECISION_FP64) return cudaErrorInvalidValue;
+        return launch_sweep_split(a, precision, c.layout, s);
+    }
     const bool mix = precision == TVS_PRECISION_MIXED64;
     const bool f64 = precision == TVS_PRECISION_FP64;
     if (!f64 && !mix && precision != TVS_PRECISION_EXACT32) return cudaErrorInvalidValue;
-    if (!queue_config_valid(c)) return cudaErrorInvalidValue;
-    if (c.layout != 0 && f64) return cudaErrorInvalidValue;
+    if (a.rings) return cudaErrorInvalidValue;  // ring records come from the split layouts
     const bool packed = c.packed && !f64 && !mix;
     const bool pipe = c.prefetch && !packed;
     // ctl + {steps, byte offsets} + FP64 double tables or packed exact-f32 tables
-    // (32 B each); the direction-split layouts instead take 8 B per step and the
-    // forward surfaces (8 B per point of view of the CTA)
+    // (32 B each)
     const bool wide = f64 || mix || packed;
     const size_t smem =
-        c.layout ? sizeof(QueueCtl) +
-                       (size_t)a.max_step_cap * (sizeof(float4) + 2 * sizeof(long long)) +
-                       (size_t)(a.max_step_cap + kSegSteps - 1) / kSegSteps * sizeof(SegBound) +
-                       (size_t)kThreads * kSplitCols * (sizeof(double) + (mix ? sizeof(int32_t) : 0))
-                 : sizeof(QueueCtl) +
-                       (size_t)a.max_step_cap * (sizeof(float4) + sizeof(long long) + (wide ? 32 : 0));
+        row_ctl_bytes() + (size_t)a.max_step_cap * (sizeof(float4) + sizeof(long long) + (wide ? 32 : 0));
 #define TVS_Q(X, Y)                                                                         \
     if (c.px == X && c.py == Y)                                                             \
         return mix ? (pipe ? launch_queue_t<TVS_PRECISION_MIXED64, X, Y, 2>(a, smem, s)      \
@@ -1140,12 +685,6 @@ cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, const QueueCon
                : packed ? launch_queue_t<TVS_PRECISION_EXACT32, X, Y, 1>(a, smem, s)        \
                : pipe ? launch_queue_t<TVS_PRECISION_EXACT32, X, Y, 2>(a, smem, s)          \
                       : launch_queue_t<TVS_PRECISION_EXACT32, X, Y, 0>(a, smem, s);
-#define TVS_L(L)                                                                  \
-    if (c.layout == L)                                                            \
-        return mix ? launch_queue_t<TVS_PRECISION_MIXED64, 1, 1, L + 2>(a, smem, s) \
-                   : launch_queue_t<TVS_PRECISION_EXACT32, 1, 1, L + 2>(a, smem, s);
-    TVS_L(1) TVS_L(2) TVS_L(3) TVS_L(4) TVS_L(5) TVS_L(6)
-#undef TVS_L
     TVS_Q(1, 1) TVS_Q(2, 1) TVS_Q(4, 1) TVS_Q(2, 2) TVS_Q(8, 1)
 #undef TVS_Q
     return cudaErrorInvalidValue;

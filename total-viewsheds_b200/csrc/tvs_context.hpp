@@ -48,6 +48,10 @@ struct tvs_context {
     uint4 *d_spill = nullptr;
     uint32_t *d_counters = nullptr;
     uint32_t spill_cap = 0;
+    uint64_t ring_capacity = 0;                // u32 slots in d_rings
+    tvs::QueueDem *d_qdem_rings = nullptr;     // this context tiled for the ring sweep
+    uint32_t ring_layout = 0;                  // the ring sweep's split layout
+    uint32_t q_ring_tiles = 0;
     // plain-kernel scratch (allocated on first use)
     float *d_sf = nullptr, *d_sb = nullptr;
     // band shapes installed as tables (the reference's shape cache), in place of
@@ -62,6 +66,16 @@ struct tvs_context {
     uint32_t *d_rc_ids = nullptr;
     uint64_t rc_ids_cap = 0, rc_total = 0;
     bool rc_valid = false;
+    // sweep counters (tvs_set_sweep_counters): [0] warp-steps swept, [1] past
+    // the first test, [2] in all, [3] spare
+    unsigned long long *d_diag = nullptr;
+    bool diag_on = false;
+    // the whole-TVS pipeline (tvs_device_run_tvs): one captured graph, and the
+    // events it records at the start, after the shape stage and at the end
+    cudaGraph_t tvs_graph = nullptr;
+    cudaGraphExec_t tvs_exec = nullptr;
+    cudaEvent_t ev_begin = nullptr, ev_shaped = nullptr, ev_swept = nullptr;
+    uint64_t tvs_graph_launches = 0;  // kernels inside the graph
     // sectors whose shape stage ran since the last tvs_device_finish
     bool pending[tvs::kSectorSteps] = {};
     uint64_t device_bytes = 0;  // everything this context allocated on the device
@@ -75,4 +89,5 @@ tvs::QueueDem queue_dem_of(const tvs_context *c);
 int header_status_of(tvs_context *c, uint32_t first, uint32_t count);
 int fail_of(tvs_context *c, int code, const std::string &msg);
 int enqueue_shape_of(tvs_context *c, uint32_t first, uint32_t count);
+void drop_tvs_graph_of(tvs_context *c);
 }  // namespace tvs_host

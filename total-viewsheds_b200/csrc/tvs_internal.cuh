@@ -118,7 +118,8 @@ struct SweepArgs {
     double *cumulative64;          // MIXED64/FP64 accumulation (nullable)
     // Ring output (one sector per launch when non-null).
     uint32_t *rings;
-    uint32_t reserved;
+    uint32_t reserved;             // slots per band in `rings`
+    uint32_t ref_reserved;         // the reference's slots per band (overflow statistics)
     uint64_t half_bands;           // computable_points_count
     uint4 *spill;                  // {kernel id lo, kernel id hi, slot, value}
     uint32_t spill_cap;
@@ -162,7 +163,21 @@ struct QueueArgs {
     uint32_t held_tile;                // failure-detection test hook: this tile
                                        // counter (done_base + tile) never advances
                                        // (0xFFFFFFFF: none)
-    unsigned long long *rechecks;      // MIXED64: FP64 re-decisions (nullable)
+    unsigned long long *rechecks;      // re-decided comparisons (nullable)
+    // Ring records of the direction-split sweeps (nullable; one sector per
+    // launch): band k's count at rings[k * ring_reserved], its ids in slots
+    // 1 .. ring_reserved - 1, further ids as {k lo, k hi, slot, id} in spill.
+    uint32_t *rings;
+    uint32_t ring_reserved;            // slots per band in `rings`
+    uint32_t ref_reserved;             // the reference's slots per band (statistics)
+    uint64_t half_bands;               // computable points of the whole grid
+    uint4 *spill;
+    uint32_t spill_cap;
+    uint32_t *ring_counters;           // [0] spill entries [1] bands past ref_reserved
+                                       // [2] most ids in one band
+    // Diagnostics (nullable): [0] warp-steps swept, [1] warp-steps past the
+    // first test, [2] warp-steps of the fast loop in all, [3] spare.
+    unsigned long long *diag;
 };
 
 // Points of view per thread (columns px 32 apart, rows py 8 apart), the
@@ -235,9 +250,16 @@ cudaError_t launch_sweep_const(const SweepArgs &a, int precision, uint32_t n_ste
 cudaError_t launch_sweep_plain(const PlainArgs &a, cudaStream_t s);
 cudaError_t launch_sweep_queue(const QueueArgs &a, int precision, const QueueConfig &c,
                                cudaStream_t s);
+// The direction-split layouts 1-6 (sweep_split.cu): EXACT32, MIXED64 and
+// FP32; ring records when a.rings is set (one sector).
+cudaError_t launch_sweep_split(const QueueArgs &a, int precision, int layout, cudaStream_t s);
+size_t split_smem_bytes(int precision, uint32_t step_cap);
 uint32_t queue_tiles_bound(uint32_t tvs_width, uint32_t rows);
 bool queue_config_valid(const QueueConfig &c);
 QueueConfig default_queue_config(int precision);
+// The precision's default direction-split layout (for the ring sweep when the
+// context's own configuration is a row layout).
+QueueConfig default_split_config(int precision);
 // Sets tiles_x/tiles_y/tile_base/done_base of every DEM for the configuration.
 void queue_tile(QueueDem *dems, uint32_t n_dems, const QueueConfig &c, uint32_t *tiles_per_sector,
                 uint32_t *done_total);
@@ -246,6 +268,7 @@ cudaError_t launch_shape_batch(const ShapeArgs *d_args, uint32_t n_dems, uint32_
 cudaError_t launch_combine(float *cum, float *total, const float *sf, const float *sb,
                            uint64_t n, cudaStream_t s);
 cudaError_t measure_fp32_issue(double *instructions_per_second);
+cudaError_t measure_l1_load(double *bytes_per_second);
 // y[i] = (double)x[i]
 cudaError_t launch_widen(const float *x, double *y, uint64_t n, cudaStream_t s);
 // out[0] = max |x[i]| + |add| over n floats (out must hold 1 float).

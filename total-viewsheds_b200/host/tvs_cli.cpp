@@ -70,7 +70,7 @@ void usage() {
         "  --output-dir <DIR>             heatmap.png goes here [default: ./]\n"
         "  --scale <METRES>               override the DEM point spacing\n"
         "  --reference-observer-height    use the reference binary's hard-coded 1.8 m\n"
-        "  --precision <exact32|mixed64|fp64>  sweep arithmetic [default: exact32]\n"
+        "  --precision <exact32|mixed64|fp64|fp32>  sweep arithmetic [default: exact32]\n"
         "  --state-directory <DIR>        shape cache root [default: the OS state directory]\n"
         "  --no-cache                     neither read nor write the shape cache\n"
         "  --heatmap <every-sector|final> heatmap.png cadence [default: every-sector]\n"
@@ -263,6 +263,7 @@ int main(int argc, char **argv) {
     p.observer_height = o.reference_observer_height ? 1.8f : o.observer_height;
     p.precision = o.precision == "fp64"      ? TVS_PRECISION_FP64
                   : o.precision == "mixed64" ? TVS_PRECISION_MIXED64
+                  : o.precision == "fp32"    ? TVS_PRECISION_FP32
                                              : TVS_PRECISION_EXACT32;
     p.sweep_kernel = TVS_SWEEP_ENGINE;
     p.device = o.device;
