@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define TVS_ABI_VERSION 3
+#define TVS_ABI_VERSION 4
 
 /* Status codes.  Negative values are errors; tvs_last_error() has the text. */
 enum tvs_status {
