@@ -315,6 +315,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-rings", action="store_true")
     ap.add_argument("--shard", default="dems", choices=["dems", "rows"],
                     help="N>1: every rank its own DEM (weak scaling, default) or one DEM's "
                          "rows split over the ranks (strong scaling)")
@@ -526,6 +527,37 @@ def main():
         legs["exact32_engine"]["identical_to_plain_port"] = bool(np.array_equal(
             outs["exact32_engine"].view(np.uint32), outs["plain_port"].view(np.uint32)))
 
+    # Ring records of a whole TVS through the compact stream (one
+    # tvs_compute_sector_rings call per sector: the surfaces, the records of
+    # every band kept on the device); host-timed, every call synchronises.
+    rings_leg = None
+    if not args.no_rings and args.kernel == "engine" and rows is None:
+        cum_r = np.zeros(eng.count, np.float32)
+        total_ids = ctypes.c_uint64()
+        st = tvs.SectorStats()
+        L = tvs.lib()
+        L.tvs_compute_sector_rings(eng.ctx, 0, tvs._ptr(cum_r), ctypes.byref(total_ids),
+                                   ctypes.byref(st))  # allocates the record buffers
+        cum_r[:] = 0
+        ids_all, most = 0, 0
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for a in range(SECTORS):
+            rc = L.tvs_compute_sector_rings(eng.ctx, a, tvs._ptr(cum_r), ctypes.byref(total_ids),
+                                            ctypes.byref(st))
+            if rc:
+                raise tvs.TvsError(rc, L.tvs_last_error(eng.ctx).decode())
+            ids_all += total_ids.value
+            most = max(most, st.max_ring_ids)
+        t_rings = time.perf_counter() - t0
+        rings_leg = {"s_per_tvs": t_rings, "ids_per_tvs": ids_all,
+                     "record_bytes_per_tvs": 4 * ids_all + 8 * (g.total_bands + 1) * SECTORS,
+                     "most_ids_in_a_band": most,
+                     "vs_surfaces_only": t_rings / (total_ms / args.steps * 1e-3),
+                     "path": "tvs_compute_sector_rings per sector: H2D + D2H of the surfaces, "
+                             "shape stage, split sweep writing ring slots, scan + gather into "
+                             "the compact stream (host-timed)"}
+
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(cfg, z, g)
@@ -600,6 +632,7 @@ def main():
             "roofline": roof,
             "cpu_baseline": base, "e2e": e2e, "gpu_launches": gpu_launches,
             **({"row_split": gathered} if gathered else {}),
+            **({"rings_compact": rings_leg} if rings_leg else {}),
             **legs,
             "clocks": clk,
         }
