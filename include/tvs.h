@@ -264,7 +264,7 @@ int tvs_set_queue_wait(tvs_context *ctx, uint32_t spin_limit, uint32_t held_tile
 
 /* Sweep counters of the direction-split layouts, for roofline accounting (no
  * counterpart in the reference).  enable != 0 zeroes them and counts the
- * later sweeps; read gives [0] warp-steps swept (not skipped by the segment
+ * later sweeps, 0 stops counting (the counts stay readable); read gives [0] warp-steps swept (not skipped by the segment
  * bounds), [1] warp-steps that passed the first test, [2] warp-steps of the
  * table-division loop in all (swept or skipped), [3] 0. */
 int tvs_set_sweep_counters(tvs_context *ctx, int enable);

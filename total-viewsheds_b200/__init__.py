@@ -377,7 +377,8 @@ class Engine:
 
     def sweep_counters(self, enable=None):
         """Read the direction-split sweep counters ([swept, passed, all, 0]
-        warp-steps); enable=True/False first zeroes them and turns counting on/off."""
+        warp-steps); enable=True first zeroes them and turns counting on,
+        enable=False turns it off (the counts are kept)."""
         if enable is not None:
             self._check(lib().tvs_set_sweep_counters(self.ctx, 1 if enable else 0))
         v = (ctypes.c_uint64 * 4)()

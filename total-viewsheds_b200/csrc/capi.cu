@@ -1140,7 +1140,8 @@ int tvs_set_queue_wait(tvs_context *ctx, uint32_t spin_limit, uint32_t held_tile
 int tvs_set_sweep_counters(tvs_context *ctx, int enable) {
     if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
     TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
-    TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_diag, 0, 4 * sizeof(unsigned long long), ctx->stream));
+    if (enable)
+        TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_diag, 0, 4 * sizeof(unsigned long long), ctx->stream));
     if ((enable != 0) != ctx->diag_on) drop_tvs_graph(ctx);
     ctx->diag_on = enable != 0;
     return TVS_OK;
