@@ -1,6 +1,7 @@
 """Precision report of the precision form (3601^2 DEM, 1200-cell line of sight,
 180 sectors): how far the exact-f32 engine (bit-identical to the reference's
-f32 CPU path) and the MIXED64 engine are from the all-FP64 sweep.
+f32 CPU path), the MIXED64 engine and the reciprocal-table FP32 form are from
+the all-FP64 sweep.
 
     python total-viewsheds_b200/precision_report.py [--sectors 0,1,45,46,90]
 
@@ -8,7 +9,8 @@ Per point of view: the relative error of the cumulative surface after 180
 sectors, |x - x64| / |x64|, as p50 / p99 / max (points with x64 == 0 excluded).
 Per sector (the listed ones): ring records compared band by band; a band
 whose open/close ids differ is a ring-boundary disagreement.  MIXED64 decides
-every comparison as the FP64 sweep does, so its rings are the FP64 rings.
+every comparison as the FP64 sweep does, so its rings are the FP64 rings; they
+are compared too, as are the FP32 form's.
 Prints one JSON object.
 """
 
@@ -68,7 +70,7 @@ def main():
     out = {"workload": f"{args.config}: {w}x{w} DEM, LOS {los} m, 180 sectors, observer "
                        f"{cfg['observer_height']} m"}
     cum, timing = {}, {}
-    for p in ("fp64", "mixed64", "exact32"):
+    for p in ("fp64", "mixed64", "exact32", "fp32"):
         with tvs.Engine(z, w, s, los, observer_height=cfg["observer_height"],
                         rings_per_km=args.rings_per_km, precision=p) as eng:
             t0 = time.perf_counter()
@@ -80,35 +82,40 @@ def main():
     out["surface_rel_error_vs_fp64"] = {
         "exact32 (= reference f32 CPU path)": rel_error_stats(cum["exact32"], cum["fp64"]),
         "mixed64": rel_error_stats(cum["mixed64"], cum["fp64"]),
+        "fp32 (reciprocal-table form)": rel_error_stats(cum["fp32"], cum["fp64"]),
     }
     out["surface_rel_error_vs_cpu_f32_path"] = {
         "mixed64": rel_error_stats(cum["mixed64"], cum["exact32"]),
         "fp64": rel_error_stats(cum["fp64"], cum["exact32"]),
     }
     sectors = [int(x) for x in args.sectors.split(",") if x]
-    rings = {}
-    with tvs.Engine(z, w, s, los, observer_height=cfg["observer_height"],
-                    rings_per_km=args.rings_per_km, precision="exact32") as e32, \
-            tvs.Engine(z, w, s, los, observer_height=cfg["observer_height"],
-                       rings_per_km=args.rings_per_km, precision="fp64") as e64:
-        reserved = e32.geometry.reserved_rings_per_band
-        n = e32.geometry.ring_slots_per_sector
+    engines = {p: tvs.Engine(z, w, s, los, observer_height=cfg["observer_height"],
+                             rings_per_km=args.rings_per_km, precision=p)
+               for p in ("fp64", "exact32", "mixed64", "fp32")}
+    try:
+        reserved = engines["fp64"].geometry.reserved_rings_per_band
+        n = engines["fp64"].geometry.ring_slots_per_sector
+        rings = {k: {} for k in ("exact32", "mixed64", "fp32")}
         for a in sectors:
-            r32 = np.zeros(n, np.uint32)
-            r64 = np.zeros(n, np.uint32)
+            recs, stats = {}, {}
             try:
-                c = np.zeros(e32.count, np.float32)
-                st32 = e32.compute_sector(a, c, r32)
-                c = np.zeros(e64.count, np.float32)
-                e64.compute_sector(a, c, r64)
+                for p, e in engines.items():
+                    recs[p] = np.zeros(n, np.uint32)
+                    stats[p] = e.compute_sector(a, np.zeros(e.count, np.float32), recs[p])
             except tvs.TvsError as err:  # e.g. ring records past the buffer end
-                rings[str(a)] = {"error": str(err)}
+                for k in rings:
+                    rings[k][str(a)] = {"error": str(err)}
                 continue
-            bands, ids = ring_disagreements(r32, r64, reserved)
-            rings[str(a)] = {"bands": int(e32.geometry.total_bands), "disagreeing_bands": bands,
-                             "disagreeing_ring_slots": ids, "max_ring_ids": int(st32.max_ring_ids),
-                             "overflow_bands": int(st32.overflow_bands)}
-    out["ring_boundary_disagreements_exact32_vs_fp64"] = rings
+            for k in rings:
+                bands, ids = ring_disagreements(recs[k], recs["fp64"], reserved)
+                rings[k][str(a)] = {"bands": int(engines[k].geometry.total_bands),
+                                    "disagreeing_bands": bands, "disagreeing_ring_slots": ids,
+                                    "max_ring_ids": int(stats[k].max_ring_ids),
+                                    "overflow_bands": int(stats[k].overflow_bands)}
+    finally:
+        for e in engines.values():
+            e.close()
+    out["ring_boundary_disagreements_vs_fp64"] = rings
     print(json.dumps(out), flush=True)
 
 
