@@ -20,10 +20,7 @@ thread_local std::string g_create_error;
 
 constexpr double kRadsPerDeg = 3.14159265358979323846 / 180.0;  // Rust f64::to_radians
 constexpr double kSqrt2 = 1.41421356237309504880;               // core::f64::consts::SQRT_2
-constexpr uint32_t kSpillCap = 1u << 20;
-// Slots per band of the device buffer behind the compact ring stream: a band
-// with more ids puts the rest in the spill list (rare at this size).
-constexpr uint32_t kCompactSlots = 64;
+constexpr uint32_t kSpillCap = 1u << 22;
 
 int fail(tvs_context *ctx, int code, const std::string &msg) {
     if (ctx) ctx->err = msg; else g_create_error = msg;
@@ -250,7 +247,7 @@ SweepImpl sweep_impl() {
 }
 
 // Device ring buffer of `slots` u32 per band (the reference's reservation for
-// its layout, kCompactSlots for the compact stream), the spill list and the
+// its layout, compact_slots for the compact stream), the spill list and the
 // counters; grown when a later call needs more slots.
 int ensure_rings(tvs_context *c, uint32_t slots) {
     if (slots == 0)
@@ -379,7 +376,7 @@ int ring_queue_dem(tvs_context *c, const tvs::QueueDem **dem, uint32_t *tiles, i
 
 // Sweep sectors [first, first+count) (slots == angles).  ring_slots != 0:
 // count is 1 and the sector's ring records go to d_rings with ring_slots u32
-// per band (the reference's reservation for its layout, kCompactSlots for the
+// per band (the reference's reservation for its layout, compact_slots for the
 // compact stream).
 int enqueue_sweep(tvs_context *c, uint32_t first, uint32_t count, uint32_t ring_slots) {
     const bool rings = ring_slots != 0;
@@ -883,44 +880,56 @@ int tvs_compute_sector_rings(tvs_context *ctx, uint32_t angle, float *cumulative
     TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
     ctx->rc_valid = false;
     const uint64_t count = ctx->g.computable_points_count;
-    if (count)
-        TVS_CUDA(ctx, cudaMemcpyAsync(ctx->d_cum, cumulative_surfaces, count * sizeof(float),
-                                      cudaMemcpyHostToDevice, ctx->stream));
-    if (ctx->d_cum64 && count)
-        TVS_CUDA(ctx, tvs::launch_widen(ctx->d_cum, ctx->d_cum64, count, ctx->stream));
-    int rc = ensure_rings(ctx, kCompactSlots);
-    if (rc) return rc;
     const uint64_t bands = ctx->g.total_bands;
-    const uint32_t R = kCompactSlots;
     const uint64_t nb = tvs::ring_scan_blocks(bands);
     if (!ctx->d_rc_offsets) {
         TVS_CUDA(ctx, cudaMalloc(&ctx->d_rc_offsets, (bands + 1) * sizeof(uint64_t)));
         TVS_CUDA(ctx, cudaMalloc(&ctx->d_rc_blocks, (nb + 1) * sizeof(uint64_t)));
         ctx->device_bytes += (bands + 1 + nb + 1) * sizeof(uint64_t);
     }
-    // Every band the split sweep covers writes its count (slot 0) and its
-    // ids; the slots past a band's count are never read.  A row shard leaves
-    // the other bands unwritten (their counts must read 0), and the other
-    // sweeps write only where they have ids.
-    if (ctx->row_begin != 0 || ctx->row_end != ctx->g.tvs_height ||
-        ctx->p.sweep_kernel == TVS_SWEEP_PLAIN || ctx->p.precision == TVS_PRECISION_FP64 ||
-        sweep_impl() != SweepImpl::Queue)
-        TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_rings, 0, bands * R * sizeof(uint32_t), ctx->stream));
-    TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), ctx->stream));
-    rc = enqueue_shape(ctx, angle, 1);
+    int rc = enqueue_shape(ctx, angle, 1);
     if (rc) return rc;
     rc = header_status(ctx, angle, 1);
     if (rc) return rc;
-    rc = enqueue_sweep(ctx, angle, 1, R);
-    if (rc) return rc;
+    // The sweep writes up to `slots` ids per band in place and the rest to the
+    // spill list.  When a sector spills more than the list holds, the slots
+    // per band double and the sector runs again from the caller's surfaces (a
+    // band has at most n_steps + 2 ids, so this ends).
+    const uint32_t most = ctx->g.band_steps_filled + 4;
+    uint32_t R = 0, cnt[4];
+    uint64_t total = 0;
+    for (;;) {
+        R = std::min(ctx->compact_slots, most);
+        rc = ensure_rings(ctx, R);
+        if (rc) return rc;
+        if (count)
+            TVS_CUDA(ctx, cudaMemcpyAsync(ctx->d_cum, cumulative_surfaces, count * sizeof(float),
+                                          cudaMemcpyHostToDevice, ctx->stream));
+        if (ctx->d_cum64 && count)
+            TVS_CUDA(ctx, tvs::launch_widen(ctx->d_cum, ctx->d_cum64, count, ctx->stream));
+        // Every band the split sweep covers writes its count (slot 0) and its
+        // ids; the slots past a band's count are never read.  A row shard
+        // leaves the other bands unwritten (their counts must read 0), and the
+        // other sweeps write only where they have ids.
+        if (ctx->row_begin != 0 || ctx->row_end != ctx->g.tvs_height ||
+            ctx->p.sweep_kernel == TVS_SWEEP_PLAIN || ctx->p.precision == TVS_PRECISION_FP64 ||
+            sweep_impl() != SweepImpl::Queue)
+            TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_rings, 0, bands * R * sizeof(uint32_t), ctx->stream));
+        TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), ctx->stream));
+        rc = enqueue_sweep(ctx, angle, 1, R);
+        if (rc) return rc;
+        TVS_CUDA(ctx, cudaMemcpyAsync(cnt, ctx->d_counters, sizeof cnt, cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+        TVS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        if (cnt[0] <= ctx->spill_cap) break;
+        if (R >= most)
+            return fail(ctx, TVS_ERR_CAPACITY, "ring spill list capacity exceeded");
+        ctx->compact_slots = std::min(2 * ctx->compact_slots, most);
+    }
     if (count)
         TVS_CUDA(ctx, cudaMemcpyAsync(cumulative_surfaces, ctx->d_cum, count * sizeof(float),
                                       cudaMemcpyDeviceToHost, ctx->stream));
-    uint32_t cnt[4];
-    TVS_CUDA(ctx, cudaMemcpyAsync(cnt, ctx->d_counters, sizeof cnt, cudaMemcpyDeviceToHost,
-                                  ctx->stream));
     TVS_CUDA(ctx, tvs::launch_ring_count(ctx->d_rings, bands, R, ctx->d_rc_blocks, ctx->stream));
-    uint64_t total = 0;
     TVS_CUDA(ctx, cudaMemcpyAsync(&total, ctx->d_rc_blocks + nb, sizeof total,
                                   cudaMemcpyDeviceToHost, ctx->stream));
     TVS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -932,8 +941,6 @@ int tvs_compute_sector_rings(tvs_context *ctx, uint32_t angle, float *cumulative
         stats->max_ring_ids = cnt[2];
         stats->spill_entries = cnt[0];
     }
-    if (cnt[0] > ctx->spill_cap)
-        return fail(ctx, TVS_ERR_CAPACITY, "ring spill list capacity exceeded");
     if (total > ctx->rc_ids_cap) {
         if (ctx->d_rc_ids) {
             cudaFree(ctx->d_rc_ids);

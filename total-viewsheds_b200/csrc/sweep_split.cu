@@ -88,6 +88,17 @@ template <> struct SplitTypes<TVS_PRECISION_FP32> {
     using X = float2;  // unused
 };
 
+// MIXED64 keeps the step of each chain's maximum in shared memory (written at
+// every raise, read only by the rare re-decisions) to stay within 64
+// registers; exact f32 holds its running maximum exactly, in registers, and
+// evaluates the reference's angle wherever the first test passes.
+#ifndef TVS_MIX_J_SMEM
+#define TVS_MIX_J_SMEM 1
+#endif
+#ifndef TVS_EXACT_INLINE
+#define TVS_EXACT_INLINE 1
+#endif
+
 // Shared-memory layout of one CTA.  Every array starts on 16 bytes.
 __host__ __device__ constexpr size_t align16(size_t n) { return (n + 15) & ~(size_t)15; }
 
@@ -105,8 +116,12 @@ template <int kPrec> struct SplitSmem {
     __host__ __device__ static size_t fwd(uint32_t cap) {
         return seg(cap) + align16((size_t)((cap + kSegSteps - 1) / kSegSteps) * sizeof(SegBound));
     }
-    __host__ __device__ static size_t total(uint32_t cap) {
+    __host__ __device__ static size_t jtab(uint32_t cap) {
         return fwd(cap) + (size_t)K * kQueueThreads * sizeof(S);
+    }
+    __host__ __device__ static size_t total(uint32_t cap) {
+        return jtab(cap) + (kPrec == TVS_PRECISION_MIXED64 && TVS_MIX_J_SMEM
+                                ? (size_t)K * kQueueThreads * sizeof(int32_t) : 0);
     }
 };
 
@@ -151,6 +166,7 @@ k_sweep_split(QueueArgs a) {
     X *s_x = reinterpret_cast<X *>(smem + L::xtab(cap));
     SegBound *s_seg = reinterpret_cast<SegBound *>(smem + L::seg(cap));
     S *s_fwd = reinterpret_cast<S *>(smem + L::fwd(cap));
+    int32_t *s_j = reinterpret_cast<int32_t *>(smem + L::jtab(cap));  // MIXED64 (TVS_MIX_J_SMEM)
     const uint32_t tid = threadIdx.y * kQueueTileX + threadIdx.x;
     const uint32_t lane = threadIdx.x;
     queue_init(ctl, tid);
@@ -366,17 +382,96 @@ k_sweep_split(QueueArgs a) {
                     for (; i < n; i++) step(i);  // zero distances: y = inf, the same form
 #pragma unroll
                     for (int k = 0; k < K; k++) out[k] = sf[k];
+                } else if constexpr (!kMix && TVS_EXACT_INLINE) {
+                    // ---- exact f32, the running maximum held exactly ----------
+                    // The first test fma(e, y, -c + G) >= m - |m| 2^-19 passes
+                    // every step where a chain may change state (|a - (e y - c)|
+                    // <= 2^-22 |a| + 2^-23 c); there the reference's angle is
+                    // computed for every chain (kernel.rs:175-233).
+                    float m[K], lo[K], sf[K];
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        m[k] = kMaxAngle;
+                        lo[k] = __fmaf_rn(fabsf(m[k]), -kRel, m[k]);
+                        sf[k] = 0.0f;
+                    }
+                    for (uint32_t seg = 0; i < n_fast; seg++) {
+                        const uint32_t i1 = min(i + kSegSteps, n_fast);
+                        if (skippable(seg, [&](int k, float bound) { return bound < lo[k]; })) {
+                            i = i1;
+                            continue;
+                        }
+                        n_swept += i1 - i;
+                        TVS_UNROLL(TVS_SPLIT_UNROLL_EXACT)
+                        for (; i < i1; i++) {
+                            const float4 t = s_t[i];  // {y, -c + G, -c - G, w}
+                            const long long b = s_boff[i];
+                            float e[K];
+                            bool hit = false;
+#pragma unroll
+                            for (int k = 0; k < K; k++) {
+                                e[k] = __fsub_rn(__ldg(at(b, k)), hp32[k]);  // kernel.rs:164
+                                hit |= __fmaf_rn(e[k], t.x, t.y) >= lo[k];
+                            }
+                            if (!__any_sync(0xffffffffu, hit || prev != 0)) continue;
+                            n_passed++;
+                            const float2 x = s_x[i];  // {d, c}
+                            uint32_t vis = 0;
+#pragma unroll
+                            for (int k = 0; k < K; k++) {
+                                const float ang = __fsub_rn(div_table32(e[k], t.x, x.x), x.y);
+                                const bool v = ang > m[k];
+                                if (v) sf[k] = __fadd_rn(sf[k], t.w);
+                                m[k] = fmaxf(ang, m[k]);  // f32::max: NaN yields the other
+                                lo[k] = __fmaf_rn(fabsf(m[k]), -kRel, m[k]);
+                                vis |= (uint32_t)v << k;
+                            }
+                            if constexpr (kRings) events(vis, b);
+                        }
+                    }
+                    for (; i < n; i++) {  // the zero-distance tail, IEEE division
+                        const long long b = s_boff[i];
+                        const float2 x = s_x[i];
+                        const bool fast = x.x >= 0x1p-20f && x.x <= 0x1p20f;
+                        uint32_t vis = 0;
+#pragma unroll
+                        for (int k = 0; k < K; k++) {
+                            const float e = __fsub_rn(__ldg(at(b, k)), hp32[k]);
+                            const float ang =
+                                __fsub_rn(fast ? div_table32(e, s_t[i].x, x.x) : __fdiv_rn(e, x.x), x.y);
+                            const bool v = ang > m[k];
+                            if (v) sf[k] = __fadd_rn(sf[k], s_t[i].w);
+                            m[k] = fmaxf(ang, m[k]);
+                            vis |= (uint32_t)v << k;
+                        }
+                        if constexpr (kRings) events(vis, b);
+                    }
+#pragma unroll
+                    for (int k = 0; k < K; k++) out[k] = sf[k];
                 } else {
-                    // ---- guard band with exact re-decisions (EXACT32, MIXED64) --
+                    // ---- guard band with exact re-decisions (MIXED64) ----------
+                    constexpr bool kJSmem = kMix && TVS_MIX_J_SMEM;
                     float hi[K], lo[K];
-                    int32_t jj[K];  // step of the running maximum (-1: the initial one)
+                    // step of the running maximum (-1: the initial one)
+                    int32_t jreg[kJSmem ? 1 : K];
+                    int32_t *sj = s_j + tid;
+                    (void)jreg;
+                    (void)sj;
+                    auto getj = [&](int k) -> int32_t {
+                        if constexpr (kJSmem) return sj[k * kQueueThreads];
+                        else return jreg[k];
+                    };
+                    auto setj = [&](int k, int32_t v) {
+                        if constexpr (kJSmem) sj[k * kQueueThreads] = v;
+                        else jreg[k] = v;
+                    };
                     S acc[K];
 #pragma unroll
                     for (int k = 0; k < K; k++) {
                         // the initial maximum (-2000, exact) carries the relative part
                         hi[k] = __fmaf_rn(2000.0f, kRel, -2000.0f);
                         lo[k] = __fmaf_rn(2000.0f, -kRel, -2000.0f);
-                        jj[k] = -1;
+                        setj(k, -1);
                         acc[k] = (S)0;
                     }
                     // the exact angle of chain k at step st, in the precision's arithmetic
@@ -394,13 +489,13 @@ k_sweep_split(QueueArgs a) {
                         }
                     };
                     auto exact_max = [&](int k) -> S {
-                        const int32_t j = jj[k];
+                        const int32_t j = getj(k);
                         return j < 0 ? (S)kMaxAngle : exact_at(k, (uint32_t)j, __ldg(at(s_boff[j], k)));
                     };
                     auto raise = [&](int k, uint32_t st, float fh, float fl, const float4 &t) {
                         hi[k] = __fmaf_rn(fabsf(fh), kRel, fh);
                         lo[k] = __fmaf_rn(fabsf(fl), -kRel, fl);
-                        jj[k] = (int32_t)st;
+                        setj(k, (int32_t)st);
                         if constexpr (kMix) acc[k] = __dadd_rn(acc[k], s_x[st].y);
                         else acc[k] = __fadd_rn(acc[k], t.w);
                     };

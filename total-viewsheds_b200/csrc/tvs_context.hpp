@@ -49,6 +49,7 @@ struct tvs_context {
     uint32_t *d_counters = nullptr;
     uint32_t spill_cap = 0;
     uint64_t ring_capacity = 0;                // u32 slots in d_rings
+    uint32_t compact_slots = 64;               // slots per band behind the compact stream
     tvs::QueueDem *d_qdem_rings = nullptr;     // this context tiled for the ring sweep
     uint32_t ring_layout = 0;                  // the ring sweep's split layout
     uint32_t q_ring_tiles = 0;
