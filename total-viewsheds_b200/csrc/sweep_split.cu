@@ -98,6 +98,11 @@ template <> struct SplitTypes<TVS_PRECISION_FP32> {
 #ifndef TVS_EXACT_INLINE
 #define TVS_EXACT_INLINE 1
 #endif
+// MIXED64 re-decisions read RN64(1/d) from the shape stage's FP64 table
+// instead of recomputing it.
+#ifndef TVS_MIX_RCP_TABLE
+#define TVS_MIX_RCP_TABLE 0
+#endif
 
 // Shared-memory layout of one CTA.  Every array starts on 16 bytes.
 __host__ __device__ constexpr size_t align16(size_t n) { return (n + 15) & ~(size_t)15; }
@@ -481,7 +486,13 @@ k_sweep_split(QueueArgs a) {
                             const double hp64 = __dadd_rn((double)__ldg(ep[k / KX] + LX * (k % KX)),
                                                           (double)D.observer_height);
                             const double e = __dsub_rn((double)h, hp64);
-                            return __dsub_rn(div_table64(e, __drcp_rn(d), d), s_x[st].x);
+#if TVS_MIX_RCP_TABLE
+                            // the shape stage's RN64(1/d), read instead of recomputed
+                            const double y = __ldg(&(D.dtab + (uint64_t)(a.first_sector + s) * D.step_cap + st)->x);
+#else
+                            const double y = __drcp_rn(d);
+#endif
+                            return __dsub_rn(div_table64(e, y, d), s_x[st].x);
                         } else {
                             const float e = __fsub_rn(h, hp32[k]);
                             const float2 x = s_x[st];
