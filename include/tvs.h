@@ -277,13 +277,15 @@ int tvs_read_sweep_counters(tvs_context *ctx, uint64_t *counters);
  * of 32*points_x x 8*points_y points; packed != 0 selects the packed f32x2
  * arithmetic (exact f32 only); prefetch != 0 issues the next step's elevation
  * loads before the current step's arithmetic (not with packed).  layout
- * L in 1..6 (MIXED64 and EXACT32, with points 4x1) sweeps one direction at a
- * time, evaluating angles exactly only where a warp's filter passes: a warp
- * holds LX = 8, 16, 32 (L = 1, 2, 3 and again 4, 5, 6) columns x 32/LX rows of
- * lanes; each lane has four points of view LX columns apart (L <= 3, tiles of
- * 4 LX x 256/LX points) or 2 x 2 of them, LX columns and 32/LX rows apart
- * (L >= 4, tiles of 2 LX x 512/LX).  Defaults: layout 1 for MIXED64, 4 for
- * EXACT32, rows 2x1 for FP64.  Results do not depend on any of them. */
+ * L in 1..8 (MIXED64, EXACT32 and FP32, with points 4x1) sweeps one direction
+ * at a time, evaluating angles exactly only where a warp's first test passes:
+ * a warp holds LX = 8, 16, 32 (L = 1, 2, 3 and again 4, 5, 6; 32 and 16 for
+ * L = 7, 8) columns x 32/LX rows of lanes; each lane has four points of view
+ * LX columns apart (L <= 3, tiles of 4 LX x 256/LX points), 2 x 2 of them, LX
+ * columns and 32/LX rows apart (L = 4..6, tiles of 2 LX x 512/LX), or four of
+ * them in one column, 32/LX rows apart (L = 7, 8, tiles of LX x 1024/LX).
+ * Defaults: the fastest split layout per precision on one B200; rows 2x1 for
+ * FP64 (the only layout it runs).  Results do not depend on any of them. */
 typedef struct tvs_sweep_config {
     int32_t points_x;
     int32_t points_y;

@@ -1068,9 +1068,9 @@ int tvs_set_sweep_config(tvs_context *ctx, const tvs_sweep_config *cfg) {
     if (!tvs::queue_config_valid(c))
         return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "unsupported points-per-thread shape");
     if (c.layout != 0 && ctx->p.precision == TVS_PRECISION_FP64)
-        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "sweep layouts 1-6 are not available for FP64");
+        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "sweep layouts 1-8 are not available for FP64");
     if (c.layout == 0 && ctx->p.precision == TVS_PRECISION_FP32)
-        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "the FP32 form runs on sweep layouts 1-6 only");
+        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "the FP32 form runs on sweep layouts 1-8 only");
     if (c.px != ctx->qcfg.px || c.py != ctx->qcfg.py || c.packed != ctx->qcfg.packed ||
         c.prefetch != ctx->qcfg.prefetch || c.layout != ctx->qcfg.layout)
         drop_tvs_graph(ctx);
@@ -1101,7 +1101,7 @@ int tvs_autotune(tvs_context *ctx, uint32_t sample_sectors, tvs_sweep_config *ch
                                       {1, 1, 0, 1, 0}, {2, 1, 0, 1, 0}, {4, 1, 0, 1, 0},
                                       {2, 2, 0, 1, 0}, {4, 1, 0, 0, 1}, {4, 1, 0, 0, 2},
                                       {4, 1, 0, 0, 3}, {4, 1, 0, 0, 4}, {4, 1, 0, 0, 5},
-                                      {4, 1, 0, 0, 6}};
+                                      {4, 1, 0, 0, 6}, {4, 1, 0, 0, 7}, {4, 1, 0, 0, 8}};
     cudaEvent_t t0, t1;
     TVS_CUDA(ctx, cudaEventCreate(&t0));
     TVS_CUDA(ctx, cudaEventCreate(&t1));

@@ -21,12 +21,17 @@ constexpr int kQueueTileX = 32;
 constexpr int kQueueTileY = 8;
 constexpr int kQueueThreads = kQueueTileX * kQueueTileY;
 
-// Direction-split layouts 1-6: a warp holds LX columns x 32/LX rows of lanes;
+// Direction-split layouts 1-8: a warp holds LX columns x 32/LX rows of lanes;
 // each lane sweeps four points of view, LX columns apart (layouts 1-3: LX = 8,
-// 16, 32) or 2 x 2 of them, LX columns and 32/LX rows apart (layouts 4-6).
+// 16, 32), 2 x 2 of them, LX columns and 32/LX rows apart (layouts 4-6), or
+// four rows 32/LX apart in one column (layouts 7, 8: LX = 32, 16), so that one
+// load of the warp reads whole 128- or 64-byte rows.
 constexpr int kSplitCols = 4;  // points of view per lane
-__host__ __device__ constexpr int split_lx(int layout) { return 4 << ((layout - 1) % 3 + 1); }
-__host__ __device__ constexpr int split_ky(int layout) { return layout > 3 ? 2 : 1; }
+constexpr int kSplitLayouts = 8;
+__host__ __device__ constexpr int split_lx(int layout) {
+    return layout == 7 ? 32 : layout == 8 ? 16 : 4 << ((layout - 1) % 3 + 1);
+}
+__host__ __device__ constexpr int split_ky(int layout) { return layout > 6 ? 4 : layout > 3 ? 2 : 1; }
 __host__ __device__ constexpr int split_tile_w(int layout) {
     return kSplitCols / split_ky(layout) * split_lx(layout);
 }

@@ -23,7 +23,7 @@
 //    the table operands); forward and backward bands of a point of view run
 //    in the same loop; cum = (cum + forward) + backward keeps the reference's
 //    order.  Every step is evaluated.
-//  * Direction-split layouts 1-6 live in sweep_split.cu; launch_sweep_queue
+//  * Direction-split layouts 1-8 live in sweep_split.cu; launch_sweep_queue
 //    dispatches to them.
 //  * Steps [0, n_fast) use the table division (Markstein, see sweep.cu); the
 //    zero-distance tail uses IEEE division.
@@ -588,12 +588,12 @@ uint32_t queue_tiles_bound(uint32_t tvs_width, uint32_t rows) {
     // thin row shard gives more tiles
     auto tiles = [&](uint32_t w, uint32_t h) { return ((tvs_width + w - 1) / w) * ((rows + h - 1) / h); };
     uint32_t n = tiles(kTileX, kTileY);
-    for (int l = 1; l <= 6; l++) n = std::max(n, tiles(split_tile_w(l), split_tile_h(l)));
+    for (int l = 1; l <= kSplitLayouts; l++) n = std::max(n, tiles(split_tile_w(l), split_tile_h(l)));
     return n;
 }
 
 bool queue_config_valid(const QueueConfig &c) {
-    if (c.layout >= 1 && c.layout <= 6)
+    if (c.layout >= 1 && c.layout <= kSplitLayouts)
         return c.px == kSplitCols && c.py == 1 && !c.packed && !c.prefetch;
     if (c.layout != 0) return false;
     const int ok[][2] = {{1, 1}, {2, 1}, {4, 1}, {2, 2}, {8, 1}};
@@ -628,7 +628,7 @@ QueueConfig default_split_config(int precision) {
     auto env_layout = [](const char *name, int d) {
         const char *l = getenv(name);
         const int v = l ? atoi(l) : d;
-        return v >= 1 && v <= 6 ? v : d;
+        return v >= 1 && v <= kSplitLayouts ? v : d;
     };
     static const int mix = env_layout("TVS_SWEEP_LAYOUT", 1);
     static const int exact = env_layout("TVS_SWEEP_LAYOUT32", 4);

@@ -1,4 +1,4 @@
-// sweep_split.cu -- the direction-split persistent sweep (layouts 1-6).
+// sweep_split.cu -- the direction-split persistent sweep (layouts 1-8).
 //
 // The reference kernel (kernel.rs:153-254) walks one band of sight and keeps
 // the running maximum of angle = (h - h_pov)/d - d/R; a sample is visible
@@ -264,7 +264,7 @@ k_sweep_split(QueueArgs a) {
 #pragma unroll
             for (int k = 0; k < K; k++)
                 if (tx + LX * (k % KX) < D.tvs_width && ty + LY * (k / KX) < D.row_end) active |= 1u << k;
-            uint32_t n_swept = 0, n_passed = 0, n_rechecks = 0;  // diagnostics
+            uint32_t n_swept = 0, n_passed = 0;  // diagnostics (re-decisions count in ctl.diag[3])
             S sb[K];
 
             auto pass = [&](auto DIR) {
@@ -533,19 +533,30 @@ k_sweep_split(QueueArgs a) {
                             if (!__any_sync(0xffffffffu, hit || prev != 0)) continue;
                             n_passed++;
                             uint32_t vis = 0, amb = 0;
+                            // the surface addend of this step, read once for the four chains
+                            S w;
+                            if constexpr (kMix) w = s_x[i].y;
+                            else w = t.w;
 #pragma unroll
                             for (int k = 0; k < K; k++) {
+                                // surely visible: raise the window, without a branch
                                 const float fl = __fmaf_rn(e[k], t.x, t.z);
                                 const bool sure = fl > hi[k];
-                                if (sure) raise(k, i, fh[k], fl, t);
+                                const bool maybe = fh[k] >= lo[k];
+                                hi[k] = sure ? __fmaf_rn(fabsf(fh[k]), kRel, fh[k]) : hi[k];
+                                lo[k] = sure ? __fmaf_rn(fabsf(fl), -kRel, fl) : lo[k];
+                                if (sure) setj(k, (int32_t)i);
+                                // adding +0 leaves a non-negative sum unchanged
+                                if constexpr (kMix) acc[k] = __dadd_rn(acc[k], sure ? w : 0.0);
+                                else acc[k] = __fadd_rn(acc[k], sure ? w : 0.0f);
                                 vis |= (uint32_t)sure << k;
-                                amb |= (uint32_t)(!sure && fh[k] >= lo[k]) << k;
+                                amb |= (uint32_t)(!sure && maybe) << k;
                             }
                             if (__any_sync(0xffffffffu, amb != 0)) {
+                                if (amb) atomicAdd(&ctl.diag[3], (unsigned long long)__popc(amb));
 #pragma unroll
                                 for (int k = 0; k < K; k++) {
                                     if (!(amb >> k & 1u)) continue;
-                                    n_rechecks++;
                                     // kernel.rs:190, decided exactly
                                     if (exact_at(k, i, __ldg(at(b, k))) > exact_max(k)) {
                                         raise(k, i, fh[k], __fmaf_rn(e[k], t.x, t.z), t);
@@ -627,7 +638,6 @@ k_sweep_split(QueueArgs a) {
                     atomicAdd(&ctl.diag[1], (unsigned long long)n_passed);
                     atomicAdd(&ctl.diag[2], 2ull * n_fast);
                 }
-                if (n_rechecks) atomicAdd(&ctl.diag[3], (unsigned long long)n_rechecks);
             }
             const bool write = queue_wait_prev(a, ctl, D, s, tile, tid);  // every thread
             if (write) {
@@ -682,6 +692,8 @@ cudaError_t launch_split_layout(const QueueArgs &a, int layout, cudaStream_t s) 
     case 4: return launch_split_t<kPrec, 4, kRings>(a, s);
     case 5: return launch_split_t<kPrec, 5, kRings>(a, s);
     case 6: return launch_split_t<kPrec, 6, kRings>(a, s);
+    case 7: return launch_split_t<kPrec, 7, kRings>(a, s);
+    case 8: return launch_split_t<kPrec, 8, kRings>(a, s);
     default: return cudaErrorInvalidValue;
     }
 }
