@@ -632,7 +632,7 @@ QueueConfig default_split_config(int precision) {
     };
     static const int mix = env_layout("TVS_SWEEP_LAYOUT", 1);
     static const int exact = env_layout("TVS_SWEEP_LAYOUT32", 4);
-    static const int fp32 = env_layout("TVS_SWEEP_LAYOUT_FP32", 4);
+    static const int fp32 = env_layout("TVS_SWEEP_LAYOUT_FP32", 5);
     const int l = precision == TVS_PRECISION_MIXED64 ? mix
                   : precision == TVS_PRECISION_FP32  ? fp32
                                                      : exact;
