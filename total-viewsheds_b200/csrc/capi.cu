@@ -314,7 +314,6 @@ int enqueue_shape(tvs_context *c, uint32_t first, uint32_t count) {
 tvs::QueueDem queue_dem(const tvs_context *c) {
     tvs::QueueDem d{};
     d.elev = c->d_elev;
-    d.n_elev = c->g.size + tvs::kElevationPad;
     d.width = c->g.width;
     d.tvs_width = c->g.tvs_width;
     d.los = c->g.max_los_as_points;

@@ -44,7 +44,7 @@ __host__ __device__ constexpr int split_tile_h(int layout) {
 // over its steps, the largest and smallest 1/d and the largest first-test
 // offset.
 #ifndef TVS_SEG_STEPS
-#define TVS_SEG_STEPS 16
+#define TVS_SEG_STEPS 32
 #endif
 constexpr uint32_t kSegSteps = TVS_SEG_STEPS;
 static_assert(kSegSteps >= 1 && kSegSteps <= 32,

@@ -104,19 +104,6 @@ template <> struct SplitTypes<TVS_PRECISION_FP32> {
 #define TVS_MIX_RCP_TABLE 0
 #endif
 
-// DEM staging: each warp copies the elevations its patch of points of view
-// reads during a segment (the patch moved by the segment's offset range) into
-// shared memory with row-wise coalesced loads, and the steps read them there.
-// A segment whose footprint exceeds kStageFloats is read from global memory.
-#ifndef TVS_SPLIT_STAGE
-#define TVS_SPLIT_STAGE 1
-#endif
-#ifndef TVS_STAGE_FLOATS
-#define TVS_STAGE_FLOATS 1024
-#endif
-constexpr int kStageFloats = TVS_STAGE_FLOATS;
-constexpr bool kStage = TVS_SPLIT_STAGE != 0;
-
 // Shared-memory layout of one CTA.  Every array starts on 16 bytes.
 __host__ __device__ constexpr size_t align16(size_t n) { return (n + 15) & ~(size_t)15; }
 
@@ -137,15 +124,9 @@ template <int kPrec> struct SplitSmem {
     __host__ __device__ static size_t jtab(uint32_t cap) {
         return fwd(cap) + (size_t)K * kQueueThreads * sizeof(S);
     }
-    __host__ __device__ static size_t dxy(uint32_t cap) {
+    __host__ __device__ static size_t total(uint32_t cap) {
         return jtab(cap) + (kPrec == TVS_PRECISION_MIXED64 && TVS_MIX_J_SMEM
                                 ? (size_t)K * kQueueThreads * sizeof(int32_t) : 0);
-    }
-    __host__ __device__ static size_t stage(uint32_t cap) {
-        return dxy(cap) + (kStage ? align16((size_t)cap * sizeof(int32_t)) : 0);
-    }
-    __host__ __device__ static size_t total(uint32_t cap) {
-        return stage(cap) + (kStage ? (size_t)kQueueTileY * kStageFloats * sizeof(float) : 0);
     }
 };
 
@@ -191,9 +172,6 @@ k_sweep_split(QueueArgs a) {
     SegBound *s_seg = reinterpret_cast<SegBound *>(smem + L::seg(cap));
     S *s_fwd = reinterpret_cast<S *>(smem + L::fwd(cap));
     int32_t *s_j = reinterpret_cast<int32_t *>(smem + L::jtab(cap));  // MIXED64 (TVS_MIX_J_SMEM)
-    // staging: each step's forward offset as (dy << 16 | dx), and the warps' buffers
-    int32_t *s_dxy = reinterpret_cast<int32_t *>(smem + L::dxy(cap));
-    float *s_stage = reinterpret_cast<float *>(smem + L::stage(cap));
     const uint32_t tid = threadIdx.y * kQueueTileX + threadIdx.x;
     const uint32_t lane = threadIdx.x;
     queue_init(ctl, tid);
@@ -256,8 +234,6 @@ k_sweep_split(QueueArgs a) {
                     zmax = fmaxf(zmax, __shfl_xor_sync(0xffffffffu, zmax, o));
                 }
                 if (lane == 0) s_seg[sg] = SegBound{dx0, dx1, dy0, dy1, ymax, ymin, zmax, 0.0f};
-                if (kStage && v)  // used only where |dx|, |dy| < 2^15 (checked per segment)
-                    s_dxy[i] = (int32_t)(((uint32_t)dy << 16) | ((uint32_t)dx & 0xFFFFu));
             }
             if (tid == 0) {
                 ctl.sector_status = h->status;
@@ -374,68 +350,6 @@ k_sweep_split(QueueArgs a) {
                     }
                     return __all_sync(0xffffffffu, skip);
                 };
-                // ---- staging of a segment's footprint (kStage) ----------------
-                // The warp's chains read rows cy_r (clamped) + dy and columns
-                // cx + LX (k % KX) + dx with (dx, dy) in the segment's offset
-                // range: the box of those is copied row by row (coalesced) into
-                // the warp's buffer with a row pitch fwp = LX (mod 32), which
-                // keeps a load of the warp's LX x 32/LX lanes free of bank
-                // conflicts.  Indices outside the elevations read 0 (no lane
-                // that is kept reads them).
-                float *wbuf = s_stage + threadIdx.y * kStageFloats;
-                int fwp = 0;
-                int sbase[KY];
-                auto stage = [&](uint32_t seg) -> bool {
-                    if constexpr (!kStage) {
-                        return false;
-                    } else {
-                        const SegBound b = s_seg[seg];
-                        const int lim = 32767;
-                        if (b.dx0 < -lim || b.dx1 > lim || b.dy0 < -lim || b.dy1 > lim) return false;
-                        const int rowmax = (int)(D.row_end - 1 + D.los);
-                        const int px0 = (int)(bx * (KX * LX) + D.los), px1 = px0 + KX * LX - 1;
-                        const int py = (int)(D.row_begin + by * (kQueueTileY * LY * KY) +
-                                             threadIdx.y * LY * KY + D.los);
-                        const int py0 = min(py, rowmax), py1 = min(py + LY * KY - 1, rowmax);
-                        const int x0 = dir ? px0 - b.dx1 : px0 + b.dx0, x1 = dir ? px1 - b.dx0 : px1 + b.dx1;
-                        const int y0 = dir ? py0 - b.dy1 : py0 + b.dy0, y1 = dir ? py1 - b.dy0 : py1 + b.dy1;
-                        const int fw = x1 - x0 + 1, fh = y1 - y0 + 1;
-                        const int pitch = fw + ((LX % 32 - fw % 32) + 32) % 32;
-                        if ((long long)pitch * fh > kStageFloats) return false;
-                        __syncwarp();  // the previous segment's reads are done
-                        const long long W = D.width;
-                        for (int r = 0; r < fh; r++) {
-                            const long long row = (long long)(y0 + r) * W + x0;
-                            for (int c = (int)lane; c < fw; c += 32) {
-                                const long long at_ = row + c;
-                                wbuf[r * pitch + c] =
-                                    at_ >= 0 && (uint64_t)at_ < D.n_elev ? __ldg(D.elev + at_) : 0.0f;
-                            }
-                        }
-                        __syncwarp();
-                        fwp = pitch;
-#pragma unroll
-                        for (int r = 0; r < KY; r++) {
-                            const int cy = min((int)(ty + LY * r), (int)D.row_end - 1) + (int)D.los;
-                            sbase[r] = (cy - y0) * pitch + ((int)(tx + D.los) - x0);
-                        }
-                        return true;
-                    }
-                };
-                // the staged offset of a step: dy * pitch + dx (negated backward)
-                auto soff = [&](uint32_t st) -> int {
-                    const int p = s_dxy[st];
-                    const int o = (p >> 16) * fwp + (int)(short)(p & 0xFFFF);
-                    return dir ? -o : o;
-                };
-                // chain k's sample at a step: from the buffer (staged) or global memory
-                auto fetch = [&](auto STG, long long b, int o, int k) -> float {
-                    if constexpr (decltype(STG)::value) return wbuf[sbase[k / KX] + o + LX * (k % KX)];
-                    else return __ldg(at(b, k));
-                };
-                using Direct = std::false_type;
-                using Staged = std::true_type;
-                (void)sbase;
                 S out[K];
                 uint32_t i = 0;
                 if constexpr (kFp32) {
@@ -446,14 +360,13 @@ k_sweep_split(QueueArgs a) {
                         m[k] = kMaxAngle;
                         sf[k] = 0.0f;
                     }
-                    auto step = [&](auto STG, uint32_t st) {
+                    auto step = [&](uint32_t st) {
                         const float4 t = s_t[st];  // {y, -c, w, 0}
                         const long long b = s_boff[st];
-                        const int o = decltype(STG)::value ? soff(st) : 0;
                         uint32_t vis = 0;
 #pragma unroll
                         for (int k = 0; k < K; k++) {
-                            const float ang = __fmaf_rn(__fsub_rn(fetch(STG, b, o, k), hp32[k]), t.x, t.y);
+                            const float ang = __fmaf_rn(__fsub_rn(__ldg(at(b, k)), hp32[k]), t.x, t.y);
                             const bool v = ang > m[k];
                             if (v) sf[k] = __fadd_rn(sf[k], t.z);
                             m[k] = fmaxf(ang, m[k]);  // NaN yields the other operand
@@ -468,15 +381,10 @@ k_sweep_split(QueueArgs a) {
                             continue;
                         }
                         n_swept += i1 - i;
-                        if (stage(seg)) {
-                            TVS_UNROLL(TVS_SPLIT_UNROLL32)
-                            for (; i < i1; i++) step(Staged{}, i);
-                        } else {
-                            TVS_UNROLL(TVS_SPLIT_UNROLL32)
-                            for (; i < i1; i++) step(Direct{}, i);
-                        }
+                        TVS_UNROLL(TVS_SPLIT_UNROLL32)
+                        for (; i < i1; i++) step(i);
                     }
-                    for (; i < n; i++) step(Direct{}, i);  // zero distances: y = inf, the same form
+                    for (; i < n; i++) step(i);  // zero distances: y = inf, the same form
 #pragma unroll
                     for (int k = 0; k < K; k++) out[k] = sf[k];
                 } else if constexpr (!kMix && TVS_EXACT_INLINE) {
@@ -499,17 +407,15 @@ k_sweep_split(QueueArgs a) {
                             continue;
                         }
                         n_swept += i1 - i;
-                        auto steps = [&](auto STG) {
                         TVS_UNROLL(TVS_SPLIT_UNROLL_EXACT)
                         for (; i < i1; i++) {
                             const float4 t = s_t[i];  // {y, -c + G, -c - G, w}
                             const long long b = s_boff[i];
-                            const int o = decltype(STG)::value ? soff(i) : 0;
                             float e[K];
                             bool hit = false;
 #pragma unroll
                             for (int k = 0; k < K; k++) {
-                                e[k] = __fsub_rn(fetch(STG, b, o, k), hp32[k]);  // kernel.rs:164
+                                e[k] = __fsub_rn(__ldg(at(b, k)), hp32[k]);  // kernel.rs:164
                                 hit |= __fmaf_rn(e[k], t.x, t.y) >= lo[k];
                             }
                             if (!__any_sync(0xffffffffu, hit || prev != 0)) continue;
@@ -527,9 +433,6 @@ k_sweep_split(QueueArgs a) {
                             }
                             if constexpr (kRings) events(vis, b);
                         }
-                        };
-                        if (stage(seg)) steps(Staged{});
-                        else steps(Direct{});
                     }
                     for (; i < n; i++) {  // the zero-distance tail, IEEE division
                         const long long b = s_boff[i];
@@ -615,17 +518,15 @@ k_sweep_split(QueueArgs a) {
                         }
                         n_swept += i1 - i;
                         constexpr int kUnroll = kMix ? TVS_SPLIT_UNROLL_MIX : TVS_SPLIT_UNROLL_EXACT;
-                        auto steps = [&](auto STG) {
 #pragma unroll kUnroll
                         for (; i < i1; i++) {
                             const float4 t = s_t[i];  // {y, -c + G, -c - G, w or d}
                             const long long b = s_boff[i];
-                            const int o = decltype(STG)::value ? soff(i) : 0;
                             float e[K], fh[K];
                             bool hit = false;
 #pragma unroll
                             for (int k = 0; k < K; k++) {
-                                e[k] = __fsub_rn(fetch(STG, b, o, k), hp32[k]);  // kernel.rs:164
+                                e[k] = __fsub_rn(__ldg(at(b, k)), hp32[k]);  // kernel.rs:164
                                 fh[k] = __fmaf_rn(e[k], t.x, t.y);
                                 hit |= fh[k] >= lo[k];
                             }
@@ -665,9 +566,6 @@ k_sweep_split(QueueArgs a) {
                             }
                             if constexpr (kRings) events(vis, b);
                         }
-                        };
-                        if (stage(seg)) steps(Staged{});
-                        else steps(Direct{});
                     }
                     // the steps past the table-division domain (the zero
                     // distances): exact arithmetic from the exact maximum

@@ -130,7 +130,6 @@ struct SweepArgs {
 // One DEM of the queue: a context is a batch of one.
 struct QueueDem {
     const float *elev;
-    uint64_t n_elev;                   // floats in elev (the DEM and its padding)
     uint32_t width, tvs_width, los;
     uint32_t row_begin, row_end;
     float observer_height;
