@@ -277,13 +277,16 @@ int tvs_read_sweep_counters(tvs_context *ctx, uint64_t *counters);
  * of 32*points_x x 8*points_y points; packed != 0 selects the packed f32x2
  * arithmetic (exact f32 only); prefetch != 0 issues the next step's elevation
  * loads before the current step's arithmetic (not with packed).  layout
- * L in 1..8 (MIXED64, EXACT32 and FP32, with points 4x1) sweeps one direction
+ * L in 1..9 (MIXED64, EXACT32 and FP32, with points 4x1) sweeps one direction
  * at a time, evaluating angles exactly only where a warp's first test passes:
  * a warp holds LX = 8, 16, 32 (L = 1, 2, 3 and again 4, 5, 6; 32 and 16 for
  * L = 7, 8) columns x 32/LX rows of lanes; each lane has four points of view
  * LX columns apart (L <= 3, tiles of 4 LX x 256/LX points), 2 x 2 of them, LX
  * columns and 32/LX rows apart (L = 4..6, tiles of 2 LX x 512/LX), or four of
  * them in one column, 32/LX rows apart (L = 7, 8, tiles of LX x 1024/LX).
+ * L = 9 is L = 7's tiling read from four row-interleaved copies of the DEM
+ * (one 16-byte load per lane and step; the context holds the copies, 4x the
+ * DEM, when the DEM fits 32-bit offsets into them, else L = 9 runs as L = 7).
  * Defaults: the fastest split layout per precision on one B200; rows 2x1 for
  * FP64 (the only layout it runs).  Results do not depend on any of them. */
 typedef struct tvs_sweep_config {

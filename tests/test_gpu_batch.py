@@ -81,7 +81,7 @@ def test_sweep_configurations_agree(tvs, synth, shape):
 
 @pytest.mark.parametrize("w,h,rows", [(301, 301, None), (311, 197, None), (301, 301, (37, 90)),
                                       (301, 301, (40, 41))])
-@pytest.mark.parametrize("layout", [0, 1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("layout", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9])
 @pytest.mark.parametrize("precision,reference", [("mixed64", "fp64"), ("exact32", "exact32")])
 def test_split_layouts_agree(tvs, synth, w, h, layout, rows, precision, reference):
     """Every sweep layout (rows of lanes over both directions, and one direction
@@ -137,7 +137,7 @@ def test_engine_autotune(tvs, synth):
 
 
 @pytest.mark.parametrize("kind", ["terraces", "steep"])
-@pytest.mark.parametrize("layout", [1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("layout", [1, 2, 3, 4, 5, 6, 7, 8, 9])
 @pytest.mark.parametrize("precision,reference", [("mixed64", "fp64"), ("exact32", "exact32")])
 def test_split_layouts_on_hard_terrain(tvs, synth, kind, layout, precision, reference):
     """The filtered layouts on terrain that stresses the filter: terraces (many

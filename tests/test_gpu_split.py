@@ -33,7 +33,7 @@ def dem1201(synth):
     return synth.config_dem("plain_gpu")
 
 
-@pytest.mark.parametrize("layout", [1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("layout", [1, 2, 3, 4, 5, 6, 7, 8, 9])
 def test_fp32_form_all_sectors(tvs, oracle, dem301, layout):
     w, s, los = PLAIN_CPU
     g = oracle.geometry(w, s, los)
@@ -60,7 +60,7 @@ def test_fp32_form_flat_sea_sector(tvs, oracle, dem1201, angle):
 
 
 @pytest.mark.parametrize("precision", ["exact32", "mixed64", "fp32"])
-@pytest.mark.parametrize("layout", [1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("layout", [1, 2, 3, 4, 5, 6, 7, 8, 9])
 @pytest.mark.parametrize("rows", [None, (37, 90)])
 def test_ring_records_every_layout(tvs, oracle, dem301, precision, layout, rows):
     """The compact stream straight from the split sweep, for a whole grid and a

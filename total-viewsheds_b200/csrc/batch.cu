@@ -106,7 +106,13 @@ int enqueue_run(tvs_batch *b, uint32_t count) {
     }
     TVS_BCUDA(b, tvs::launch_shape_batch(b->d_shape, (uint32_t)b->dems.size(), tvs::kSectorSteps,
                                          b->stream));
-    TVS_BCUDA(b, tvs::launch_sweep_queue(queue_args(b, 0, count), (int)b->precision, b->cfg,
+    // the quad layout needs every DEM's row-interleaved copies, else its tiling
+    // runs from the plain DEMs
+    tvs::QueueConfig cfg = b->cfg;
+    if (cfg.layout == tvs::kQuadLayout)
+        for (const tvs_context *c : b->dems)
+            if (!c->d_quad) cfg.layout = tvs::kQuadFallback;
+    TVS_BCUDA(b, tvs::launch_sweep_queue(queue_args(b, 0, count), (int)b->precision, cfg,
                                          b->stream));
     return TVS_OK;
 }
@@ -218,9 +224,9 @@ int tvs_batch_set_sweep_config(tvs_batch *b, const tvs_sweep_config *cfg) {
     if (!tvs::queue_config_valid(c))
         return bfail(b, TVS_ERR_INVALID_ARGUMENT, "unsupported points-per-thread shape");
     if (c.layout != 0 && b->precision == TVS_PRECISION_FP64)
-        return bfail(b, TVS_ERR_INVALID_ARGUMENT, "sweep layouts 1-8 are not available for FP64");
+        return bfail(b, TVS_ERR_INVALID_ARGUMENT, "sweep layouts 1-9 are not available for FP64");
     if (c.layout == 0 && b->precision == TVS_PRECISION_FP32)
-        return bfail(b, TVS_ERR_INVALID_ARGUMENT, "the FP32 form runs on sweep layouts 1-8 only");
+        return bfail(b, TVS_ERR_INVALID_ARGUMENT, "the FP32 form runs on sweep layouts 1-9 only");
     if (c.px != b->cfg.px || c.py != b->cfg.py || c.packed != b->cfg.packed ||
         c.prefetch != b->cfg.prefetch || c.layout != b->cfg.layout) {
         b->cfg = c;
@@ -253,7 +259,8 @@ int tvs_batch_autotune(tvs_batch *b, uint32_t sample_sectors, tvs_sweep_config *
                                       {1, 1, 0, 1, 0}, {2, 1, 0, 1, 0}, {4, 1, 0, 1, 0},
                                       {2, 2, 0, 1, 0}, {4, 1, 0, 0, 1}, {4, 1, 0, 0, 2},
                                       {4, 1, 0, 0, 3}, {4, 1, 0, 0, 4}, {4, 1, 0, 0, 5},
-                                      {4, 1, 0, 0, 6}, {4, 1, 0, 0, 7}, {4, 1, 0, 0, 8}};
+                                      {4, 1, 0, 0, 6}, {4, 1, 0, 0, 7}, {4, 1, 0, 0, 8},
+                                      {4, 1, 0, 0, 9}};
     cudaEvent_t t0, t1;
     TVS_BCUDA(b, cudaEventCreate(&t0));
     TVS_BCUDA(b, cudaEventCreate(&t1));

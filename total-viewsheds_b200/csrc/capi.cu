@@ -147,7 +147,7 @@ void free_all(tvs_context *c) {
                     c->d_deltas, c->d_dists, c->d_rings, c->d_spill, c->d_counters, c->d_sf,
                     c->d_sb, c->d_tab_deltas, c->d_tab_dists, c->d_installed,
                     c->d_rc_blocks, c->d_rc_offsets, c->d_rc_ids, c->d_bmax, c->d_qdem_rings,
-                    c->d_diag};
+                    c->d_diag, c->d_quad};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     drop_tvs_graph(c);
@@ -314,6 +314,8 @@ int enqueue_shape(tvs_context *c, uint32_t first, uint32_t count) {
 tvs::QueueDem queue_dem(const tvs_context *c) {
     tvs::QueueDem d{};
     d.elev = c->d_elev;
+    d.quad = c->d_quad;
+    d.quad_copy = tvs::quad_copy_elems(c->g.width, c->g.height);
     d.width = c->g.width;
     d.tvs_width = c->g.tvs_width;
     d.los = c->g.max_los_as_points;
@@ -333,6 +335,12 @@ tvs::QueueDem queue_dem(const tvs_context *c) {
     d.bmax_w = c->bmax_w;
     d.bmax_h = c->bmax_h;
     return d;
+}
+
+// The split layout a launch runs: the quad layout needs the context's
+// row-interleaved copies, else its tiling runs from the plain DEM.
+int runnable_layout(const tvs_context *c, int layout) {
+    return layout == tvs::kQuadLayout && !c->d_quad ? tvs::kQuadFallback : layout;
 }
 
 int upload_queue_dem(tvs_context *c) {
@@ -448,7 +456,8 @@ int enqueue_sweep(tvs_context *c, uint32_t first, uint32_t count, uint32_t ring_
         q.spill = c->d_spill;
         q.spill_cap = c->spill_cap;
         q.ring_counters = c->d_counters;
-        TVS_CUDA(c, tvs::launch_sweep_split(q, (int)c->p.precision, layout, c->stream));
+        TVS_CUDA(c, tvs::launch_sweep_split(q, (int)c->p.precision, runnable_layout(c, layout),
+                                            c->stream));
         c->launches++;
         return TVS_OK;
     }
@@ -471,7 +480,9 @@ int enqueue_sweep(tvs_context *c, uint32_t first, uint32_t count, uint32_t ring_
         q.held_tile = c->held_tile;
         q.rechecks = c->d_rechecks;
         q.diag = c->diag_on ? c->d_diag : nullptr;
-        TVS_CUDA(c, tvs::launch_sweep_queue(q, (int)c->p.precision, c->qcfg, c->stream));
+        tvs::QueueConfig cfg = c->qcfg;
+        cfg.layout = runnable_layout(c, cfg.layout);
+        TVS_CUDA(c, tvs::launch_sweep_queue(q, (int)c->p.precision, cfg, c->stream));
         c->launches++;
         return TVS_OK;
     }
@@ -687,6 +698,19 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
             return bail(e, "cudaMalloc");
         c->device_bytes += count * sizeof(double);
     }
+    // the quad layout's copies (4x the DEM); without them (FP64, the plain
+    // kernel, a DEM past the 32-bit offsets, or no memory for them) the quad
+    // layout's tiling runs from the plain DEM
+    if (params->precision != TVS_PRECISION_FP64 && params->sweep_kernel == TVS_SWEEP_ENGINE &&
+        tvs::quad_fits(g.width, g.height)) {
+        const size_t qb = 4 * tvs::quad_copy_elems(g.width, g.height) * sizeof(float4);
+        if (cudaMalloc(&c->d_quad, qb) == cudaSuccess) {
+            c->device_bytes += qb;
+        } else {
+            cudaGetLastError();
+            c->d_quad = nullptr;
+        }
+    }
     // Per-sector trigonometry on the host (glibc, as Rust std on linux-gnu):
     // axes.rs:95 shifts the angle in f32, axes.rs:127 adds 90 in f32.
     std::vector<tvs::SectorTrig> trig(slots);
@@ -710,6 +734,8 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
     if ((e = tvs::launch_max_abs(c->d_elev, g.size, params->observer_height, c->d_hmax, 0)) !=
             cudaSuccess ||
         (e = tvs::launch_block_max(c->d_elev, g.width, g.height, c->d_bmax, 0)) != cudaSuccess ||
+        (c->d_quad && (e = tvs::launch_quad_copies(c->d_elev, g.width, g.height, c->d_quad, 0)) !=
+                          cudaSuccess) ||
         (e = cudaDeviceSynchronize()) != cudaSuccess)
         return bail(e, "elevation range");
     if ((e = cudaMemset(c->d_hdr, 0, slots * sizeof(tvs::ShapeHeader))) != cudaSuccess ||
@@ -751,6 +777,9 @@ int tvs_set_elevations(tvs_context *ctx, const float *elevations, uint64_t n) {
                                       ctx->stream));
     TVS_CUDA(ctx, tvs::launch_block_max(ctx->d_elev, ctx->g.width, ctx->g.height, ctx->d_bmax,
                                         ctx->stream));
+    if (ctx->d_quad)
+        TVS_CUDA(ctx, tvs::launch_quad_copies(ctx->d_elev, ctx->g.width, ctx->g.height,
+                                              ctx->d_quad, ctx->stream));
     return TVS_OK;
 }
 
@@ -1068,9 +1097,9 @@ int tvs_set_sweep_config(tvs_context *ctx, const tvs_sweep_config *cfg) {
     if (!tvs::queue_config_valid(c))
         return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "unsupported points-per-thread shape");
     if (c.layout != 0 && ctx->p.precision == TVS_PRECISION_FP64)
-        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "sweep layouts 1-8 are not available for FP64");
+        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "sweep layouts 1-9 are not available for FP64");
     if (c.layout == 0 && ctx->p.precision == TVS_PRECISION_FP32)
-        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "the FP32 form runs on sweep layouts 1-8 only");
+        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "the FP32 form runs on sweep layouts 1-9 only");
     if (c.px != ctx->qcfg.px || c.py != ctx->qcfg.py || c.packed != ctx->qcfg.packed ||
         c.prefetch != ctx->qcfg.prefetch || c.layout != ctx->qcfg.layout)
         drop_tvs_graph(ctx);
@@ -1101,7 +1130,8 @@ int tvs_autotune(tvs_context *ctx, uint32_t sample_sectors, tvs_sweep_config *ch
                                       {1, 1, 0, 1, 0}, {2, 1, 0, 1, 0}, {4, 1, 0, 1, 0},
                                       {2, 2, 0, 1, 0}, {4, 1, 0, 0, 1}, {4, 1, 0, 0, 2},
                                       {4, 1, 0, 0, 3}, {4, 1, 0, 0, 4}, {4, 1, 0, 0, 5},
-                                      {4, 1, 0, 0, 6}, {4, 1, 0, 0, 7}, {4, 1, 0, 0, 8}};
+                                      {4, 1, 0, 0, 6}, {4, 1, 0, 0, 7}, {4, 1, 0, 0, 8},
+                                      {4, 1, 0, 0, 9}};
     cudaEvent_t t0, t1;
     TVS_CUDA(ctx, cudaEventCreate(&t0));
     TVS_CUDA(ctx, cudaEventCreate(&t1));

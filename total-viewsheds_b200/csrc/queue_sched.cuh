@@ -21,15 +21,17 @@ constexpr int kQueueTileX = 32;
 constexpr int kQueueTileY = 8;
 constexpr int kQueueThreads = kQueueTileX * kQueueTileY;
 
-// Direction-split layouts 1-8: a warp holds LX columns x 32/LX rows of lanes;
+// Direction-split layouts 1-9: a warp holds LX columns x 32/LX rows of lanes;
 // each lane sweeps four points of view, LX columns apart (layouts 1-3: LX = 8,
 // 16, 32), 2 x 2 of them, LX columns and 32/LX rows apart (layouts 4-6), or
 // four rows 32/LX apart in one column (layouts 7, 8: LX = 32, 16), so that one
-// load of the warp reads whole 128- or 64-byte rows.
+// load of the warp reads whole 128- or 64-byte rows.  Layout 9 (quad) is
+// layout 7's tiling with the four rows read as one float4 from the DEM's
+// row-interleaved copies: a warp's load is 512 contiguous bytes.
 constexpr int kSplitCols = 4;  // points of view per lane
-constexpr int kSplitLayouts = 8;
+constexpr int kSplitLayouts = 9;
 __host__ __device__ constexpr int split_lx(int layout) {
-    return layout == 7 ? 32 : layout == 8 ? 16 : 4 << ((layout - 1) % 3 + 1);
+    return layout == 7 || layout == 9 ? 32 : layout == 8 ? 16 : 4 << ((layout - 1) % 3 + 1);
 }
 __host__ __device__ constexpr int split_ky(int layout) { return layout > 6 ? 4 : layout > 3 ? 2 : 1; }
 __host__ __device__ constexpr int split_tile_w(int layout) {

@@ -506,6 +506,25 @@ __global__ void k_block_max(const float *elev, uint32_t W, uint32_t H, float *bm
     bmax[b] = m;
 }
 
+// quad[c * per + g * W + x] = rows c + 4g .. c + 4g + 3 of column x (zero
+// past the DEM and in the padding after the groups).
+__global__ void k_quad_copies(const float *elev, uint32_t W, uint32_t H, uint64_t per,
+                              float4 *quad) {
+    const uint64_t n = 4 * per, groups = quad_groups(H);
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = i / per, r = i - c * per;
+        const uint64_t g = r / W, x = r - g * W;
+        float v[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const uint64_t row = c + 4 * g + q;
+            v[q] = g < groups && row < H ? elev[row * W + x] : 0.0f;
+        }
+        quad[i] = make_float4(v[0], v[1], v[2], v[3]);
+    }
+}
+
 __global__ void k_widen(const float *x, double *y, uint64_t n) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) y[i] = (double)x[i];
@@ -518,6 +537,13 @@ cudaError_t launch_block_max(const float *elev, uint32_t W, uint32_t H, float *b
     const uint32_t n = ((W + kBlockMax - 1) / kBlockMax) * ((H + kBlockMax - 1) / kBlockMax);
     if (n == 0) return cudaSuccess;
     k_block_max<<<(n + 255) / 256, 256, 0, s>>>(elev, W, H, bmax);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_quad_copies(const float *elev, uint32_t W, uint32_t H, float4 *quad,
+                               cudaStream_t s) {
+    if (W == 0 || H == 0) return cudaSuccess;
+    k_quad_copies<<<148 * 8, 256, 0, s>>>(elev, W, H, quad_copy_elems(W, H), quad);
     return cudaGetLastError();
 }
 

@@ -23,7 +23,7 @@
 //    the table operands); forward and backward bands of a point of view run
 //    in the same loop; cum = (cum + forward) + backward keeps the reference's
 //    order.  Every step is evaluated.
-//  * Direction-split layouts 1-8 live in sweep_split.cu; launch_sweep_queue
+//  * Direction-split layouts 1-9 live in sweep_split.cu; launch_sweep_queue
 //    dispatches to them.
 //  * Steps [0, n_fast) use the table division (Markstein, see sweep.cu); the
 //    zero-distance tail uses IEEE division.
@@ -631,8 +631,8 @@ QueueConfig default_split_config(int precision) {
         return v >= 1 && v <= kSplitLayouts ? v : d;
     };
     static const int mix = env_layout("TVS_SWEEP_LAYOUT", 1);
-    static const int exact = env_layout("TVS_SWEEP_LAYOUT32", 4);
-    static const int fp32 = env_layout("TVS_SWEEP_LAYOUT_FP32", 5);
+    static const int exact = env_layout("TVS_SWEEP_LAYOUT32", kQuadLayout);
+    static const int fp32 = env_layout("TVS_SWEEP_LAYOUT_FP32", kQuadLayout);
     const int l = precision == TVS_PRECISION_MIXED64 ? mix
                   : precision == TVS_PRECISION_FP32  ? fp32
                                                      : exact;

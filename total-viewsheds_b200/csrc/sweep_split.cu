@@ -1,4 +1,4 @@
-// sweep_split.cu -- the direction-split persistent sweep (layouts 1-8).
+// sweep_split.cu -- the direction-split persistent sweep (layouts 1-9).
 //
 // The reference kernel (kernel.rs:153-254) walks one band of sight and keeps
 // the running maximum of angle = (h - h_pov)/d - d/R; a sample is visible
@@ -65,6 +65,27 @@ __device__ __forceinline__ double div_table64(double e, double y, double d) {
     const double q = __dmul_rn(e, y);
     const double r = __fma_rn(-d, q, e);
     return __fma_rn(r, y, q);
+}
+
+// A step's forward DEM offset (cells) as (x, y): |x| < W/2 on every band of
+// sight, and |y| <= the line of sight (the shape stage's path check).
+__device__ __forceinline__ void step_xy(long long off, long long W, long long &dx, long long &dy) {
+    const long long q = off + W / 2;
+    dy = q >= 0 ? q / W : -((W - 1 - q) / W);
+    dx = off - dy * W;
+}
+
+// The quad layout's forward and backward byte offsets of a step from a lane's
+// base (copy 0, the group of its first row, its column): rows r0 + y .. +3
+// sit in copy (rho + y) mod 4, rho = r0 mod 4 (r0 = the lane's first row).
+__device__ __forceinline__ int2 quad_offsets(long long off, long long W, long long rho,
+                                             long long copy_bytes) {
+    long long dx, dy;
+    step_xy(off, W, dx, dy);
+    const long long cf = (rho + dy) & 3, cb = (rho - dy) & 3;
+    const long long fwd = cf * copy_bytes + (rho + dy - cf) / 4 * W * 16 + dx * 16;
+    const long long bwd = cb * copy_bytes + (rho - dy - cb) / 4 * W * 16 - dx * 16;
+    return make_int2((int)fwd, (int)bwd);
 }
 
 // The per-step window: 2^-20 (d/R + hmax/d) plus a floor, as the shape of
@@ -135,9 +156,12 @@ template <int kPrec> struct SplitSmem {
 #ifndef TVS_SPLIT_MIX_BLOCKS
 #define TVS_SPLIT_MIX_BLOCKS 4
 #endif
+#ifndef TVS_SPLIT_BLOCKS32
+#define TVS_SPLIT_BLOCKS32 4
+#endif
 template <int kPrec, bool kRings>
 constexpr int split_min_blocks() {
-    return kRings ? 3 : kPrec == TVS_PRECISION_MIXED64 ? TVS_SPLIT_MIX_BLOCKS : 4;
+    return kRings ? 3 : kPrec == TVS_PRECISION_MIXED64 ? TVS_SPLIT_MIX_BLOCKS : TVS_SPLIT_BLOCKS32;
 }
 
 // Unroll factors of the step loops (FP32 4, exact f32 4, MIXED64 1: the
@@ -160,6 +184,7 @@ k_sweep_split(QueueArgs a) {
     constexpr int LX = split_lx(kLayout), KY = split_ky(kLayout), KX = K / KY, LY = 32 / LX;
     constexpr bool kFp32 = kPrec == TVS_PRECISION_FP32;
     constexpr bool kMix = kPrec == TVS_PRECISION_MIXED64;
+    constexpr bool kQuad = kLayout == kQuadLayout;
     using L = SplitSmem<kPrec>;
     using S = typename L::S;
     using X = typename L::X;
@@ -168,6 +193,7 @@ k_sweep_split(QueueArgs a) {
     QueueCtl &ctl = *reinterpret_cast<QueueCtl *>(smem + L::ctl());
     float4 *s_t = reinterpret_cast<float4 *>(smem + L::steps(cap));
     long long *s_boff = reinterpret_cast<long long *>(smem + L::boff(cap));
+    int2 *s_q = reinterpret_cast<int2 *>(smem + L::boff(cap));  // quad: {forward, backward}
     X *s_x = reinterpret_cast<X *>(smem + L::xtab(cap));
     SegBound *s_seg = reinterpret_cast<SegBound *>(smem + L::seg(cap));
     S *s_fwd = reinterpret_cast<S *>(smem + L::fwd(cap));
@@ -191,7 +217,11 @@ k_sweep_split(QueueArgs a) {
             const float hmax = kFp32 ? 0.0f : *D.hmax;
             for (uint32_t i = tid; i < n; i += kQueueThreads) {
                 const float4 t = gs[i];  // {RN(1/d), d, RN(d/R), RN(d*tan1)}
-                s_boff[i] = (long long)go[i].x * (long long)sizeof(float);
+                if constexpr (kQuad)
+                    s_q[i] = quad_offsets(go[i].x, D.width, (D.row_begin + D.los) & 3u,
+                                          (long long)D.quad_copy * 16);
+                else
+                    s_boff[i] = (long long)go[i].x * (long long)sizeof(float);
                 if constexpr (kFp32) {
                     s_t[i] = make_float4(t.x, -t.z, t.w, 0.0f);
                 } else {
@@ -214,11 +244,9 @@ k_sweep_split(QueueArgs a) {
             for (uint32_t sg = threadIdx.y; sg * kSegSteps < nf; sg += kQueueTileY) {
                 const uint32_t i = sg * kSegSteps + lane;
                 const bool v = lane < kSegSteps && i < nf;
-                // the step's forward offset as (x, y): |x| < W/2 on every band of sight
-                const long long off = v ? s_boff[i] / (long long)sizeof(float) : 0;
-                const long long q = off + W / 2;
-                const long long dy = q >= 0 ? q / W : -((W - 1 - q) / W);
-                const int dx = (int)(off - dy * W);
+                long long dxl, dy;
+                step_xy(v ? (long long)go[i].x : 0, W, dxl, dy);
+                const int dx = (int)dxl;
                 int dx0 = v ? dx : INT_MAX, dx1 = v ? dx : INT_MIN;
                 int dy0 = v ? (int)dy : INT_MAX, dy1 = v ? (int)dy : INT_MIN;
                 float ymax = v ? s_t[i].x : -INFINITY, ymin = v ? s_t[i].x : INFINITY;
@@ -256,6 +284,18 @@ k_sweep_split(QueueArgs a) {
 #pragma unroll
             for (int r = 0; r < KY; r++)
                 ep[r] = D.elev + (int64_t)(min(ty + LY * r, D.row_end - 1) + D.los) * D.width + tx + D.los;
+            // quad: the lane's base in the row-interleaved copies (rows past the
+            // grid are not clamped: the copies hold zero rows for them)
+            const char *qbase = nullptr;
+            if constexpr (kQuad)
+                qbase = reinterpret_cast<const char *>(
+                    D.quad + (uint64_t)((ty + D.los - ((D.row_begin + D.los) & 3u)) / 4) * D.width +
+                    tx + D.los);
+            const int2 *goff = D.offs + (uint64_t)(a.first_sector + s) * D.step_cap;
+            const double4 *gdt = D.dtab + (uint64_t)(a.first_sector + s) * D.step_cap;  // MIXED64
+            (void)qbase;
+            (void)goff;
+            (void)gdt;
             float hp32[K];  // kernel.rs:134, the f32 observer elevation
 #pragma unroll
             for (int k = 0; k < K; k++)
@@ -273,6 +313,34 @@ k_sweep_split(QueueArgs a) {
                     return (const float *)((const char *)ep[k / KX] + (dir ? -b : b)) + LX * (k % KX);
                 };
                 // ring records of chain k: kernel id and the DEM id of a sample
+                // the four chains' samples at step st
+                auto load = [&](uint32_t st, float (&h)[K]) {
+                    if constexpr (kQuad) {
+                        const int2 o = s_q[st];
+                        const float4 v = __ldg(reinterpret_cast<const float4 *>(qbase + (dir ? o.y : o.x)));
+                        h[0] = v.x;
+                        h[1] = v.y;
+                        h[2] = v.z;
+                        h[3] = v.w;
+                    } else {
+                        const long long b = s_boff[st];
+#pragma unroll
+                        for (int k = 0; k < K; k++) h[k] = __ldg(at(b, k));
+                    }
+                };
+                auto load1 = [&](uint32_t st, int k) -> float {
+                    if constexpr (kQuad) {
+                        const int2 o = s_q[st];
+                        return __ldg(reinterpret_cast<const float *>(qbase + (dir ? o.y : o.x)) + k);
+                    } else {
+                        return __ldg(at(s_boff[st], k));
+                    }
+                };
+                // the step's forward offset in bytes in the DEM (ring ids)
+                auto orig = [&](uint32_t st) -> long long {
+                    if constexpr (kQuad) return (long long)__ldg(&goff[st].x) * (long long)sizeof(float);
+                    else return s_boff[st];
+                };
                 auto kid = [&](int k) -> uint64_t {
                     return (uint64_t)(ty + LY * (k / KX)) * D.tvs_width + tx + LX * (k % KX) +
                            (dir ? a.half_bands : 0);
@@ -302,9 +370,10 @@ k_sweep_split(QueueArgs a) {
                 } else {
                     prev = 0;
                 }
-                auto events = [&](uint32_t vis, long long b) {
+                auto events = [&](uint32_t vis, uint32_t st) {
                     const uint32_t ev = (vis ^ prev) & active;
                     if (__any_sync(0xffffffffu, ev != 0)) {
+                        const long long b = orig(st);
 #pragma unroll
                         for (int k = 0; k < K; k++)
                             if (ev >> k & 1u) ring_put(kid(k), ++nr[k], dem_id(k, b));
@@ -362,17 +431,18 @@ k_sweep_split(QueueArgs a) {
                     }
                     auto step = [&](uint32_t st) {
                         const float4 t = s_t[st];  // {y, -c, w, 0}
-                        const long long b = s_boff[st];
+                        float h[K];
+                        load(st, h);
                         uint32_t vis = 0;
 #pragma unroll
                         for (int k = 0; k < K; k++) {
-                            const float ang = __fmaf_rn(__fsub_rn(__ldg(at(b, k)), hp32[k]), t.x, t.y);
+                            const float ang = __fmaf_rn(__fsub_rn(h[k], hp32[k]), t.x, t.y);
                             const bool v = ang > m[k];
                             if (v) sf[k] = __fadd_rn(sf[k], t.z);
                             m[k] = fmaxf(ang, m[k]);  // NaN yields the other operand
                             vis |= (uint32_t)v << k;
                         }
-                        if constexpr (kRings) events(vis, b);
+                        if constexpr (kRings) events(vis, st);
                     };
                     for (uint32_t seg = 0; i < n_fast; seg++) {
                         const uint32_t i1 = min(i + kSegSteps, n_fast);
@@ -410,12 +480,12 @@ k_sweep_split(QueueArgs a) {
                         TVS_UNROLL(TVS_SPLIT_UNROLL_EXACT)
                         for (; i < i1; i++) {
                             const float4 t = s_t[i];  // {y, -c + G, -c - G, w}
-                            const long long b = s_boff[i];
                             float e[K];
+                            load(i, e);
                             bool hit = false;
 #pragma unroll
                             for (int k = 0; k < K; k++) {
-                                e[k] = __fsub_rn(__ldg(at(b, k)), hp32[k]);  // kernel.rs:164
+                                e[k] = __fsub_rn(e[k], hp32[k]);  // kernel.rs:164
                                 hit |= __fmaf_rn(e[k], t.x, t.y) >= lo[k];
                             }
                             if (!__any_sync(0xffffffffu, hit || prev != 0)) continue;
@@ -431,17 +501,18 @@ k_sweep_split(QueueArgs a) {
                                 lo[k] = __fmaf_rn(fabsf(m[k]), -kRel, m[k]);
                                 vis |= (uint32_t)v << k;
                             }
-                            if constexpr (kRings) events(vis, b);
+                            if constexpr (kRings) events(vis, i);
                         }
                     }
                     for (; i < n; i++) {  // the zero-distance tail, IEEE division
-                        const long long b = s_boff[i];
                         const float2 x = s_x[i];
                         const bool fast = x.x >= 0x1p-20f && x.x <= 0x1p20f;
+                        float h[K];
+                        load(i, h);
                         uint32_t vis = 0;
 #pragma unroll
                         for (int k = 0; k < K; k++) {
-                            const float e = __fsub_rn(__ldg(at(b, k)), hp32[k]);
+                            const float e = __fsub_rn(h[k], hp32[k]);
                             const float ang =
                                 __fsub_rn(fast ? div_table32(e, s_t[i].x, x.x) : __fdiv_rn(e, x.x), x.y);
                             const bool v = ang > m[k];
@@ -449,7 +520,7 @@ k_sweep_split(QueueArgs a) {
                             m[k] = fmaxf(ang, m[k]);
                             vis |= (uint32_t)v << k;
                         }
-                        if constexpr (kRings) events(vis, b);
+                        if constexpr (kRings) events(vis, i);
                     }
 #pragma unroll
                     for (int k = 0; k < K; k++) out[k] = sf[k];
@@ -458,7 +529,7 @@ k_sweep_split(QueueArgs a) {
                     constexpr bool kJSmem = kMix && TVS_MIX_J_SMEM;
                     float hi[K], lo[K];
                     // step of the running maximum (-1: the initial one)
-                    int32_t jreg[kJSmem ? 1 : K];
+                    int32_t jreg[kJSmem ? 1 : K] = {};
                     int32_t *sj = s_j + tid;
                     (void)jreg;
                     (void)sj;
@@ -488,7 +559,7 @@ k_sweep_split(QueueArgs a) {
                             const double e = __dsub_rn((double)h, hp64);
 #if TVS_MIX_RCP_TABLE
                             // the shape stage's RN64(1/d), read instead of recomputed
-                            const double y = __ldg(&(D.dtab + (uint64_t)(a.first_sector + s) * D.step_cap + st)->x);
+                            const double y = __ldg(&gdt[st].x);
 #else
                             const double y = __drcp_rn(d);
 #endif
@@ -501,7 +572,7 @@ k_sweep_split(QueueArgs a) {
                     };
                     auto exact_max = [&](int k) -> S {
                         const int32_t j = getj(k);
-                        return j < 0 ? (S)kMaxAngle : exact_at(k, (uint32_t)j, __ldg(at(s_boff[j], k)));
+                        return j < 0 ? (S)kMaxAngle : exact_at(k, (uint32_t)j, load1((uint32_t)j, k));
                     };
                     auto raise = [&](int k, uint32_t st, float fh, float fl, const float4 &t) {
                         hi[k] = __fmaf_rn(fabsf(fh), kRel, fh);
@@ -521,12 +592,12 @@ k_sweep_split(QueueArgs a) {
 #pragma unroll kUnroll
                         for (; i < i1; i++) {
                             const float4 t = s_t[i];  // {y, -c + G, -c - G, w or d}
-                            const long long b = s_boff[i];
                             float e[K], fh[K];
+                            load(i, e);
                             bool hit = false;
 #pragma unroll
                             for (int k = 0; k < K; k++) {
-                                e[k] = __fsub_rn(__ldg(at(b, k)), hp32[k]);  // kernel.rs:164
+                                e[k] = __fsub_rn(e[k], hp32[k]);  // kernel.rs:164
                                 fh[k] = __fmaf_rn(e[k], t.x, t.y);
                                 hit |= fh[k] >= lo[k];
                             }
@@ -558,13 +629,13 @@ k_sweep_split(QueueArgs a) {
                                 for (int k = 0; k < K; k++) {
                                     if (!(amb >> k & 1u)) continue;
                                     // kernel.rs:190, decided exactly
-                                    if (exact_at(k, i, __ldg(at(b, k))) > exact_max(k)) {
+                                    if (exact_at(k, i, load1(i, k)) > exact_max(k)) {
                                         raise(k, i, fh[k], __fmaf_rn(e[k], t.x, t.z), t);
                                         vis |= 1u << k;
                                     }
                                 }
                             }
-                            if constexpr (kRings) events(vis, b);
+                            if constexpr (kRings) events(vis, i);
                         }
                     }
                     // the steps past the table-division domain (the zero
@@ -573,11 +644,12 @@ k_sweep_split(QueueArgs a) {
 #pragma unroll
                     for (int k = 0; k < K; k++) m[k] = exact_max(k);
                     for (; i < n; i++) {
-                        const long long b = s_boff[i];
+                        float hk[K];
+                        load(i, hk);
                         uint32_t vis = 0;
 #pragma unroll
                         for (int k = 0; k < K; k++) {
-                            const float h = __ldg(at(b, k));
+                            const float h = hk[k];
                             S ang;
                             if constexpr (kMix) {
                                 const double d = (double)s_t[i].w;
@@ -599,7 +671,7 @@ k_sweep_split(QueueArgs a) {
                             else m[k] = fmaxf(ang, m[k]);  // f32::max: NaN yields the other
                             vis |= (uint32_t)v << k;
                         }
-                        if constexpr (kRings) events(vis, b);
+                        if constexpr (kRings) events(vis, i);
                     }
 #pragma unroll
                     for (int k = 0; k < K; k++) out[k] = acc[k];
@@ -607,7 +679,7 @@ k_sweep_split(QueueArgs a) {
                 if constexpr (kRings) {
                     // kernel.rs:237-243: close a ring cut off by the line of
                     // sight, then the count in slot 0
-                    const long long b_last = n ? s_boff[n - 1] : 0;
+                    const long long b_last = n ? orig(n - 1) : 0;
                     uint32_t most = 0, over = 0;
 #pragma unroll
                     for (int k = 0; k < K; k++) {
@@ -694,6 +766,7 @@ cudaError_t launch_split_layout(const QueueArgs &a, int layout, cudaStream_t s) 
     case 6: return launch_split_t<kPrec, 6, kRings>(a, s);
     case 7: return launch_split_t<kPrec, 7, kRings>(a, s);
     case 8: return launch_split_t<kPrec, 8, kRings>(a, s);
+    case 9: return launch_split_t<kPrec, 9, kRings>(a, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -724,10 +797,34 @@ cudaError_t launch_persistent(const void *fn, const QueueArgs &a, size_t smem, c
             o.attr = smem;
         }
         if (o.blocks < 0 || o.smem != smem) {
-            int b = 0;
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kQueueThreads, smem);
+            // The resident CTAs at the largest shared-memory carveout, then the
+            // smallest carveout that still holds them: the rest of the SM's
+            // 256 KB stays L1 cache for the DEM samples (left to itself the
+            // driver sizes the carveout for more CTAs than the registers allow).
+            int b = 0, per_sm = 0, reserved = 0;
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+            if (e == cudaSuccess)
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kQueueThreads, smem);
+            if (e == cudaSuccess)
+                e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+            if (e == cudaSuccess)
+                e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
             if (e != cudaSuccess) return e;
-            o.blocks = b < 1 ? 1 : b;
+            b = b < 1 ? 1 : b;
+            if (per_sm > 0) {
+                const size_t need = (size_t)b * (smem + (size_t)reserved);
+                const int pct = (int)std::min<size_t>(100, (need * 100 + per_sm - 1) / per_sm);
+                int b2 = 0;
+                e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+                if (e == cudaSuccess)
+                    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, fn, kQueueThreads, smem);
+                if (e != cudaSuccess) return e;
+                if (b2 < b) {  // the rounding lost a CTA: keep the largest carveout
+                    e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+                    if (e != cudaSuccess) return e;
+                }
+            }
+            o.blocks = b;
             o.smem = smem;
         }
         blocks_per_sm = o.blocks;

@@ -33,6 +33,7 @@ struct tvs_context {
     int32_t *d_error = nullptr;
     float *d_hmax = nullptr;  // max |elevation| + |observer height| (estimate windows)
     float *d_bmax = nullptr;  // block maxima of the elevations (segment bounds)
+    float4 *d_quad = nullptr; // row-interleaved copies (the quad split layout), nullable
     uint32_t bmax_w = 0, bmax_h = 0;
     unsigned long long *d_rechecks = nullptr;  // MIXED64 FP64 re-decisions
     tvs::QueueDem *d_qdem = nullptr;           // this context as a one-DEM queue

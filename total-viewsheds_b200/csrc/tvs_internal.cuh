@@ -28,6 +28,25 @@ constexpr float kEarthRadiusSquared = 12742000.0f;
 #endif
 constexpr uint32_t kBlockMax = TVS_BLOCK_MAX;
 
+// Four row-interleaved copies of a DEM for the quad split layout: copy c
+// holds rows c + 4g .. c + 4g + 3 of group g as one float4 per column, so the
+// four points of view of a lane, in consecutive rows, read one aligned 16-byte
+// vector at every step whatever the step's row offset.  Rows past the DEM are
+// zero; the groups reach the rows that a tile past the grid's last row
+// addresses (up to H + 30), and kQuadPad float4 after them the columns past a
+// row's end.  The sweep's step offsets are 32-bit byte offsets, so the four
+// copies must lie within 2^31 bytes (quad_fits).
+constexpr int kQuadLayout = 9;     // the split layout that reads them
+constexpr int kQuadFallback = 7;   // the same tiling from the plain DEM
+constexpr uint32_t kQuadPad = 64;
+__host__ __device__ constexpr uint32_t quad_groups(uint32_t height) { return (height + 48) / 4 + 2; }
+__host__ __device__ constexpr uint64_t quad_copy_elems(uint32_t width, uint32_t height) {
+    return ((uint64_t)quad_groups(height) * width + kQuadPad + 15) & ~(uint64_t)15;
+}
+__host__ __device__ constexpr bool quad_fits(uint32_t width, uint32_t height) {
+    return 4 * quad_copy_elems(width, height) * 16 < (1ull << 31);
+}
+
 #ifdef __CUDACC__
 // The FP64 sweep's per-step values from the step's f32 distance d
 // (kernel.rs:175,216 in double): {1/d, d/R, d*tan1, d}.  The shape stage
@@ -130,6 +149,8 @@ struct SweepArgs {
 // One DEM of the queue: a context is a batch of one.
 struct QueueDem {
     const float *elev;
+    const float4 *quad;                // the row-interleaved copies (nullable)
+    uint64_t quad_copy;                // float4 per copy
     uint32_t width, tvs_width, los;
     uint32_t row_begin, row_end;
     float observer_height;
@@ -233,6 +254,9 @@ cudaError_t launch_ring_gather(const uint32_t *rings, uint64_t bands, uint32_t r
 // (NaN ignored; -inf for an all-NaN block).
 cudaError_t launch_block_max(const float *elev, uint32_t width, uint32_t height, float *bmax,
                              cudaStream_t s);
+// The quad layout's copies of a width x height DEM (4 * quad_copy_elems float4).
+cudaError_t launch_quad_copies(const float *elev, uint32_t width, uint32_t height, float4 *quad,
+                               cudaStream_t s);
 cudaError_t launch_shape_tables(const ShapeArgs &a, uint32_t n_sectors, const int32_t *tab_deltas,
                                 const float *tab_dists, const unsigned char *installed,
                                 cudaStream_t s);
