@@ -166,3 +166,36 @@ def test_sweep_counters(tvs, synth, precision):
 def test_peak_probes(tvs):
     assert tvs.measure_fp32_issue(0) > 1e13      # FFMA lane-instructions / s
     assert tvs.measure_l1_load(0) > 1e12         # bytes / s
+
+
+@pytest.mark.parametrize("precision", ["exact32", "mixed64", "fp32"])
+def test_quad_layout_wide_steps(tvs, oracle, synth, precision):
+    """A short line of sight on a wide DEM: at many angles a step moves a point
+    of view more than the line of sight sideways, so the reference's linear
+    sample ids wrap rows (kernel.rs:259-292).  The quad layout reads the plain
+    DEM for those sectors; surfaces and ring records equal the oracle's at
+    every angle whose bands stay on the DEM."""
+    z = synth.fbm(101, 101, 0.8, 4, 0.0, 100.0)
+    w, s, los = 101, 1.0, 10
+    g = oracle.geometry(w, s, los)
+    swept = 0
+    with tvs.Engine(z, w, s, los, observer_height=1.65, precision=precision) as eng:
+        eng.set_sweep_config(4, 1, layout=9)
+        for angle in range(0, 180, 5):
+            try:
+                d, x, _ = oracle.compile_band_data(g, float(angle))
+                c0, n0, ids0 = oracle.sweep_sector(g, z, 1.65, d, x, mode=ORACLE_MODE[precision],
+                                                   compact=True)
+            except oracle.OracleError as e:
+                assert e.code == -4
+                with pytest.raises(tvs.TvsError) as err:
+                    eng.compute_sector(angle, np.zeros(eng.count, np.float32))
+                assert err.value.code == tvs.ERR_PATH_OUT_OF_DEM
+                continue
+            cum = np.zeros(eng.count, np.float32)
+            offsets, ids, _ = eng.compute_sector_rings(angle, cum)
+            assert np.array_equal(bits(cum), bits(f32(c0))), angle
+            assert np.array_equal(np.diff(offsets).astype(np.uint32), n0), angle
+            assert np.array_equal(ids, ids0), angle
+            swept += 1
+    assert swept > 0

@@ -67,6 +67,7 @@ struct QueueCtl {
     uint32_t n_steps;
     uint32_t n_fast;
     bool restage;
+    bool plain;             // quad layout: the staged sector reads the plain DEM
     float hmax;             // the staged DEM's elevation range (estimate windows)
     unsigned long long diag[4];  // per-item counters (sweep_split.cu), flushed per item
 };

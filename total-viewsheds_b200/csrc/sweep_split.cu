@@ -215,9 +215,26 @@ k_sweep_split(QueueArgs a) {
             const int2 *go = D.offs + (uint64_t)slot * D.step_cap;
             const double4 *gd = D.dtab + (uint64_t)slot * D.step_cap;
             const float hmax = kFp32 ? 0.0f : *D.hmax;
+            // The quad copies hold a lane's four rows at one column.  The
+            // reference's sample ids are linear (kernel.rs:259-292), so a step
+            // that moves more than the line of sight sideways wraps a point of
+            // view's row; such a sector reads the plain DEM.  Otherwise every
+            // point of view's samples stay on its own rows, inside the DEM, and
+            // every quad address inside the copies.
+            bool plain = !kQuad;
+            if constexpr (kQuad) {
+                bool wide = false;
+                for (uint32_t i = tid; i < n; i += kQueueThreads) {
+                    long long dx, dy;
+                    step_xy(go[i].x, D.width, dx, dy);
+                    wide |= dx > (long long)D.los || dx < -(long long)D.los;
+                }
+                plain = __syncthreads_or(wide) != 0;
+                if (tid == 0) ctl.plain = plain;
+            }
             for (uint32_t i = tid; i < n; i += kQueueThreads) {
                 const float4 t = gs[i];  // {RN(1/d), d, RN(d/R), RN(d*tan1)}
-                if constexpr (kQuad)
+                if (!plain)
                     s_q[i] = quad_offsets(go[i].x, D.width, (D.row_begin + D.los) & 3u,
                                           (long long)D.quad_copy * 16);
                 else
@@ -307,15 +324,19 @@ k_sweep_split(QueueArgs a) {
             uint32_t n_swept = 0, n_passed = 0;  // diagnostics (re-decisions count in ctl.diag[3])
             S sb[K];
 
-            auto pass = [&](auto DIR) {
+            // one direction's sweep; PLAIN: a quad-layout sector that reads the
+            // plain DEM (a separate instantiation, so that the quad loop is as
+            // lean as without it)
+            auto pass = [&](auto DIR, auto PLAIN) {
                 constexpr int dir = decltype(DIR)::value;
+                constexpr bool qplain = decltype(PLAIN)::value;
                 auto at = [&](long long b, int k) -> const float * {
                     return (const float *)((const char *)ep[k / KX] + (dir ? -b : b)) + LX * (k % KX);
                 };
                 // ring records of chain k: kernel id and the DEM id of a sample
                 // the four chains' samples at step st
                 auto load = [&](uint32_t st, float (&h)[K]) {
-                    if constexpr (kQuad) {
+                    if constexpr (kQuad && !qplain) {
                         const int2 o = s_q[st];
                         const float4 v = __ldg(reinterpret_cast<const float4 *>(qbase + (dir ? o.y : o.x)));
                         h[0] = v.x;
@@ -329,7 +350,7 @@ k_sweep_split(QueueArgs a) {
                     }
                 };
                 auto load1 = [&](uint32_t st, int k) -> float {
-                    if constexpr (kQuad) {
+                    if constexpr (kQuad && !qplain) {
                         const int2 o = s_q[st];
                         return __ldg(reinterpret_cast<const float *>(qbase + (dir ? o.y : o.x)) + k);
                     } else {
@@ -338,8 +359,10 @@ k_sweep_split(QueueArgs a) {
                 };
                 // the step's forward offset in bytes in the DEM (ring ids)
                 auto orig = [&](uint32_t st) -> long long {
-                    if constexpr (kQuad) return (long long)__ldg(&goff[st].x) * (long long)sizeof(float);
-                    else return s_boff[st];
+                    if constexpr (kQuad && !qplain)
+                        return (long long)__ldg(&goff[st].x) * (long long)sizeof(float);
+                    else
+                        return s_boff[st];
                 };
                 auto kid = [&](int k) -> uint64_t {
                     return (uint64_t)(ty + LY * (k / KX)) * D.tvs_width + tx + LX * (k % KX) +
@@ -702,8 +725,21 @@ k_sweep_split(QueueArgs a) {
                     else sb[k] = out[k];
                 }
             };
-            pass(std::integral_constant<int, 0>{});
-            pass(std::integral_constant<int, 1>{});
+            using Fwd = std::integral_constant<int, 0>;
+            using Bwd = std::integral_constant<int, 1>;
+            using Quad = std::false_type;
+            if constexpr (kQuad) {
+                if (ctl.plain) {
+                    pass(Fwd{}, std::true_type{});
+                    pass(Bwd{}, std::true_type{});
+                } else {
+                    pass(Fwd{}, Quad{});
+                    pass(Bwd{}, Quad{});
+                }
+            } else {
+                pass(Fwd{}, Quad{});
+                pass(Bwd{}, Quad{});
+            }
             if (a.diag || a.rechecks) {
                 if (lane == 0) {
                     atomicAdd(&ctl.diag[0], (unsigned long long)n_swept);
