@@ -199,3 +199,25 @@ def test_quad_layout_wide_steps(tvs, oracle, synth, precision):
             assert np.array_equal(ids, ids0), angle
             swept += 1
     assert swept > 0
+
+
+def test_mixed64_lean_form_long_line_of_sight(tvs, oracle, synth):
+    """A 1900-cell line of sight: MIXED64's per-step tables would hold fewer
+    CTAs per SM than the register limit, so its surfaces run the lean form (the
+    maximum's step in registers, the FP64 addend recomputed from d).  Bit for
+    bit the FP64 oracle, on several layouts."""
+    w, s, los = 3900, 30.0, 57000
+    z = synth.fbm(w, w, 0.8, 21, 0.0, 3000.0)
+    g = oracle.geometry(w, s, los)
+    assert g.max_los_as_points == 1900 and g.tvs_width == 100
+    want = {}
+    for angle in (0, 46, 90):
+        d, x, _ = oracle.compile_band_data(g, float(angle))
+        want[angle] = oracle.sweep_sector(g, z, 1.65, d, x, mode="fp64")[0]
+    with tvs.Engine(z, w, s, los, observer_height=1.65, precision="mixed64") as eng:
+        for layout in (1, 5, 9):
+            eng.set_sweep_config(4, 1, layout=layout)
+            for angle, c0 in want.items():
+                cum = np.zeros(eng.count, np.float32)
+                eng.compute_sector(angle, cum)
+                assert np.array_equal(bits(cum), bits(f32(c0))), (layout, angle)

@@ -109,13 +109,16 @@ template <> struct SplitTypes<TVS_PRECISION_FP32> {
     using X = float2;  // unused
 };
 
-// MIXED64 keeps the step of each chain's maximum in shared memory (written at
-// every raise, read only by the rare re-decisions) to stay within 64
-// registers; exact f32 holds its running maximum exactly, in registers, and
-// evaluates the reference's angle wherever the first test passes.
-#ifndef TVS_MIX_J_SMEM
-#define TVS_MIX_J_SMEM 1
-#endif
+// MIXED64 comes in two forms (kLean).  The default keeps the step of each
+// chain's maximum in shared memory (written at every raise, read only by the
+// rare re-decisions) to stay within 64 registers, and stages {RN64(d/R),
+// RN64(d*0.0174533)} per step.  The lean form, for lines of sight whose
+// tables would leave fewer than three CTAs per SM, holds the maximum's step in
+// registers, recomputes the surface addend from the staged f32 d (one DMUL,
+// the shape stage's own operation) and reads RN64(d/R) for the rare exact
+// re-decisions from the FP64 table in global memory.  Exact f32 holds its
+// running maximum exactly, in registers, and evaluates the reference's angle
+// wherever the first test passes.
 #ifndef TVS_EXACT_INLINE
 #define TVS_EXACT_INLINE 1
 #endif
@@ -128,10 +131,11 @@ template <> struct SplitTypes<TVS_PRECISION_FP32> {
 // Shared-memory layout of one CTA.  Every array starts on 16 bytes.
 __host__ __device__ constexpr size_t align16(size_t n) { return (n + 15) & ~(size_t)15; }
 
-template <int kPrec> struct SplitSmem {
+template <int kPrec, bool kLean = false> struct SplitSmem {
     using S = typename SplitTypes<kPrec>::S;
     using X = typename SplitTypes<kPrec>::X;
-    static constexpr bool kExactTab = kPrec != TVS_PRECISION_FP32;
+    static constexpr bool kExactTab =
+        kPrec == TVS_PRECISION_EXACT32 || (kPrec == TVS_PRECISION_MIXED64 && !kLean);
     __host__ __device__ static size_t ctl() { return 0; }
     __host__ __device__ static size_t steps(uint32_t) { return align16(sizeof(QueueCtl)); }
     __host__ __device__ static size_t boff(uint32_t cap) { return steps(cap) + align16((size_t)cap * 16); }
@@ -146,7 +150,7 @@ template <int kPrec> struct SplitSmem {
         return fwd(cap) + (size_t)K * kQueueThreads * sizeof(S);
     }
     __host__ __device__ static size_t total(uint32_t cap) {
-        return jtab(cap) + (kPrec == TVS_PRECISION_MIXED64 && TVS_MIX_J_SMEM
+        return jtab(cap) + (kPrec == TVS_PRECISION_MIXED64 && !kLean
                                 ? (size_t)K * kQueueThreads * sizeof(int32_t) : 0);
     }
 };
@@ -178,14 +182,14 @@ constexpr int split_min_blocks() {
 #define TVS_PRAGMA(x) _Pragma(#x)
 #define TVS_UNROLL(n) TVS_PRAGMA(unroll n)
 
-template <int kPrec, int kLayout, bool kRings>
+template <int kPrec, int kLayout, bool kRings, bool kLean>
 __global__ void __launch_bounds__(kQueueThreads, (split_min_blocks<kPrec, kRings>()))
 k_sweep_split(QueueArgs a) {
     constexpr int LX = split_lx(kLayout), KY = split_ky(kLayout), KX = K / KY, LY = 32 / LX;
     constexpr bool kFp32 = kPrec == TVS_PRECISION_FP32;
     constexpr bool kMix = kPrec == TVS_PRECISION_MIXED64;
     constexpr bool kQuad = kLayout == kQuadLayout;
-    using L = SplitSmem<kPrec>;
+    using L = SplitSmem<kPrec, kLean>;
     using S = typename L::S;
     using X = typename L::X;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -197,7 +201,7 @@ k_sweep_split(QueueArgs a) {
     X *s_x = reinterpret_cast<X *>(smem + L::xtab(cap));
     SegBound *s_seg = reinterpret_cast<SegBound *>(smem + L::seg(cap));
     S *s_fwd = reinterpret_cast<S *>(smem + L::fwd(cap));
-    int32_t *s_j = reinterpret_cast<int32_t *>(smem + L::jtab(cap));  // MIXED64 (TVS_MIX_J_SMEM)
+    int32_t *s_j = reinterpret_cast<int32_t *>(smem + L::jtab(cap));  // MIXED64, not lean
     const uint32_t tid = threadIdx.y * kQueueTileX + threadIdx.x;
     const uint32_t lane = threadIdx.x;
     queue_init(ctl, tid);
@@ -247,7 +251,7 @@ k_sweep_split(QueueArgs a) {
                     if constexpr (kMix) {
                         s_t[i] = make_float4(t.x, zhi, zlo, t.y);
                         const double4 dt = gd[i];  // {1/d, d/R, d*tan1, d} in double
-                        s_x[i] = make_double2(dt.y, dt.z);
+                        if constexpr (L::kExactTab) s_x[i] = make_double2(dt.y, dt.z);
                     } else {
                         s_t[i] = make_float4(t.x, zhi, zlo, t.w);
                         s_x[i] = make_float2(t.y, t.z);
@@ -549,7 +553,7 @@ k_sweep_split(QueueArgs a) {
                     for (int k = 0; k < K; k++) out[k] = sf[k];
                 } else {
                     // ---- guard band with exact re-decisions (MIXED64) ----------
-                    constexpr bool kJSmem = kMix && TVS_MIX_J_SMEM;
+                    constexpr bool kJSmem = kMix && !kLean;
                     float hi[K], lo[K];
                     // step of the running maximum (-1: the initial one)
                     int32_t jreg[kJSmem ? 1 : K] = {};
@@ -574,6 +578,16 @@ k_sweep_split(QueueArgs a) {
                         acc[k] = (S)0;
                     }
                     // the exact angle of chain k at step st, in the precision's arithmetic
+                    // MIXED64's per-step FP64 values (fp64_step of the staged d):
+                    // the surface addend RN64(d*0.0174533) and RN64(d/R)
+                    auto mix_w = [&](uint32_t st) -> double {
+                        if constexpr (L::kExactTab) return (double)s_x[st].y;
+                        else return __dmul_rn((double)s_t[st].w, 0.0174533);
+                    };
+                    auto mix_c = [&](uint32_t st) -> double {
+                        if constexpr (L::kExactTab) return (double)s_x[st].x;
+                        else return __ldg(&gdt[st].y);
+                    };
                     auto exact_at = [&](int k, uint32_t st, float h) -> S {
                         if constexpr (kMix) {
                             const double d = (double)s_t[st].w;
@@ -586,7 +600,7 @@ k_sweep_split(QueueArgs a) {
 #else
                             const double y = __drcp_rn(d);
 #endif
-                            return __dsub_rn(div_table64(e, y, d), s_x[st].x);
+                            return __dsub_rn(div_table64(e, y, d), mix_c(st));
                         } else {
                             const float e = __fsub_rn(h, hp32[k]);
                             const float2 x = s_x[st];
@@ -601,7 +615,7 @@ k_sweep_split(QueueArgs a) {
                         hi[k] = __fmaf_rn(fabsf(fh), kRel, fh);
                         lo[k] = __fmaf_rn(fabsf(fl), -kRel, fl);
                         setj(k, (int32_t)st);
-                        if constexpr (kMix) acc[k] = __dadd_rn(acc[k], s_x[st].y);
+                        if constexpr (kMix) acc[k] = __dadd_rn(acc[k], mix_w(st));
                         else acc[k] = __fadd_rn(acc[k], t.w);
                     };
                     for (uint32_t seg = 0; i < n_fast; seg++) {
@@ -629,7 +643,7 @@ k_sweep_split(QueueArgs a) {
                             uint32_t vis = 0, amb = 0;
                             // the surface addend of this step, read once for the four chains
                             S w;
-                            if constexpr (kMix) w = s_x[i].y;
+                            if constexpr (kMix) w = mix_w(i);
                             else w = t.w;
 #pragma unroll
                             for (int k = 0; k < K; k++) {
@@ -678,7 +692,7 @@ k_sweep_split(QueueArgs a) {
                                 const double d = (double)s_t[i].w;
                                 const double hp64 = __dadd_rn((double)__ldg(ep[k / KX] + LX * (k % KX)),
                                                               (double)D.observer_height);
-                                ang = __dsub_rn(__ddiv_rn(__dsub_rn((double)h, hp64), d), s_x[i].x);
+                                ang = __dsub_rn(__ddiv_rn(__dsub_rn((double)h, hp64), d), mix_c(i));
                             } else {
                                 const float2 x = s_x[i];
                                 const bool fast = x.x >= 0x1p-20f && x.x <= 0x1p20f;
@@ -687,7 +701,7 @@ k_sweep_split(QueueArgs a) {
                             }
                             const bool v = ang > m[k];
                             if (v) {
-                                if constexpr (kMix) acc[k] = __dadd_rn(acc[k], s_x[i].y);
+                                if constexpr (kMix) acc[k] = __dadd_rn(acc[k], mix_w(i));
                                 else acc[k] = __fadd_rn(acc[k], s_t[i].w);
                             }
                             if constexpr (kMix) m[k] = fmax(ang, m[k]);
@@ -784,27 +798,46 @@ k_sweep_split(QueueArgs a) {
     }
 }
 
-template <int kPrec, int kLayout, bool kRings>
+template <int kPrec, int kLayout, bool kRings, bool kLean>
 cudaError_t launch_split_t(const QueueArgs &a, cudaStream_t s) {
-    const size_t smem = SplitSmem<kPrec>::total(a.max_step_cap);
-    return launch_persistent(reinterpret_cast<const void *>(&k_sweep_split<kPrec, kLayout, kRings>),
-                             a, smem, s);
+    const size_t smem = SplitSmem<kPrec, kLean>::total(a.max_step_cap);
+    return launch_persistent(
+        reinterpret_cast<const void *>(&k_sweep_split<kPrec, kLayout, kRings, kLean>), a, smem, s);
 }
 
-template <int kPrec, bool kRings>
+template <int kPrec, bool kRings, bool kLean = false>
 cudaError_t launch_split_layout(const QueueArgs &a, int layout, cudaStream_t s) {
     switch (layout) {
-    case 1: return launch_split_t<kPrec, 1, kRings>(a, s);
-    case 2: return launch_split_t<kPrec, 2, kRings>(a, s);
-    case 3: return launch_split_t<kPrec, 3, kRings>(a, s);
-    case 4: return launch_split_t<kPrec, 4, kRings>(a, s);
-    case 5: return launch_split_t<kPrec, 5, kRings>(a, s);
-    case 6: return launch_split_t<kPrec, 6, kRings>(a, s);
-    case 7: return launch_split_t<kPrec, 7, kRings>(a, s);
-    case 8: return launch_split_t<kPrec, 8, kRings>(a, s);
-    case 9: return launch_split_t<kPrec, 9, kRings>(a, s);
+    case 1: return launch_split_t<kPrec, 1, kRings, kLean>(a, s);
+    case 2: return launch_split_t<kPrec, 2, kRings, kLean>(a, s);
+    case 3: return launch_split_t<kPrec, 3, kRings, kLean>(a, s);
+    case 4: return launch_split_t<kPrec, 4, kRings, kLean>(a, s);
+    case 5: return launch_split_t<kPrec, 5, kRings, kLean>(a, s);
+    case 6: return launch_split_t<kPrec, 6, kRings, kLean>(a, s);
+    case 7: return launch_split_t<kPrec, 7, kRings, kLean>(a, s);
+    case 8: return launch_split_t<kPrec, 8, kRings, kLean>(a, s);
+    case 9: return launch_split_t<kPrec, 9, kRings, kLean>(a, s);
     default: return cudaErrorInvalidValue;
     }
+}
+
+// MIXED64 surfaces run the lean form when it keeps more CTAs per SM (up to
+// the register limit) than the default form's tables allow.
+cudaError_t mix_lean(uint32_t step_cap, bool *lean) {
+    int dev = 0, per_sm = 0, reserved = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    if (e != cudaSuccess) return e;
+    auto ctas = [&](size_t smem) {
+        return std::min<size_t>(split_min_blocks<TVS_PRECISION_MIXED64, false>(),
+                                (size_t)per_sm / (smem + (size_t)reserved));
+    };
+    *lean = ctas(SplitSmem<TVS_PRECISION_MIXED64, true>::total(step_cap)) >
+            ctas(SplitSmem<TVS_PRECISION_MIXED64>::total(step_cap));
+    return cudaSuccess;
 }
 
 }  // namespace
@@ -896,9 +929,14 @@ cudaError_t launch_sweep_split(const QueueArgs &a, int precision, int layout, cu
     case TVS_PRECISION_EXACT32:
         return rings ? launch_split_layout<TVS_PRECISION_EXACT32, true>(a, layout, s)
                      : launch_split_layout<TVS_PRECISION_EXACT32, false>(a, layout, s);
-    case TVS_PRECISION_MIXED64:
-        return rings ? launch_split_layout<TVS_PRECISION_MIXED64, true>(a, layout, s)
-                     : launch_split_layout<TVS_PRECISION_MIXED64, false>(a, layout, s);
+    case TVS_PRECISION_MIXED64: {
+        if (rings) return launch_split_layout<TVS_PRECISION_MIXED64, true>(a, layout, s);
+        bool lean = false;
+        const cudaError_t e = mix_lean(a.max_step_cap, &lean);
+        if (e != cudaSuccess) return e;
+        return lean ? launch_split_layout<TVS_PRECISION_MIXED64, false, true>(a, layout, s)
+                    : launch_split_layout<TVS_PRECISION_MIXED64, false>(a, layout, s);
+    }
     case TVS_PRECISION_FP32:
         return rings ? launch_split_layout<TVS_PRECISION_FP32, true>(a, layout, s)
                      : launch_split_layout<TVS_PRECISION_FP32, false>(a, layout, s);
