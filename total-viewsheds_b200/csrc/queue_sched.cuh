@@ -18,7 +18,12 @@
 namespace tvs {
 
 constexpr int kQueueTileX = 32;
-constexpr int kQueueTileY = 8;
+// warps per CTA of the persistent sweeps (one build-wide value: the host tiles
+// the grid with it)
+#ifndef TVS_QUEUE_WARPS
+#define TVS_QUEUE_WARPS 8
+#endif
+constexpr int kQueueTileY = TVS_QUEUE_WARPS;
 constexpr int kQueueThreads = kQueueTileX * kQueueTileY;
 
 // Direction-split layouts 1-9: a warp holds LX columns x 32/LX rows of lanes;

@@ -165,7 +165,8 @@ template <int kPrec, bool kLean = false> struct SplitSmem {
 #endif
 template <int kPrec, bool kRings>
 constexpr int split_min_blocks() {
-    return kRings ? 3 : kPrec == TVS_PRECISION_MIXED64 ? TVS_SPLIT_MIX_BLOCKS : TVS_SPLIT_BLOCKS32;
+    return (kRings ? 3 : kPrec == TVS_PRECISION_MIXED64 ? TVS_SPLIT_MIX_BLOCKS : TVS_SPLIT_BLOCKS32) *
+           8 / kQueueTileY;
 }
 
 // Unroll factors of the step loops (FP32 4, exact f32 4, MIXED64 1: the
