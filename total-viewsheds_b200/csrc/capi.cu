@@ -639,6 +639,11 @@ int tvs_create(const tvs_params *params, const float *elevations, uint64_t n_ele
     if (params->device < 0 || params->device >= ndev)
         return fail(nullptr, TVS_ERR_NO_DEVICE, "device ordinal out of range");
 
+    // the MIXED64 sweep keeps the step of each chain's maximum in 16 bits
+    if (params->precision == TVS_PRECISION_MIXED64 && params->sweep_kernel == TVS_SWEEP_ENGINE &&
+        g.band_steps_filled + 2 > 0xffffu)
+        return fail(nullptr, TVS_ERR_INVALID_ARGUMENT,
+                    "MIXED64 supports band tables of up to 65535 steps");
     tvs_context *c = new tvs_context();
     c->p = *params;
     c->g = g;

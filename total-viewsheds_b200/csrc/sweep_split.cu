@@ -109,16 +109,16 @@ template <> struct SplitTypes<TVS_PRECISION_FP32> {
     using X = float2;  // unused
 };
 
-// MIXED64 comes in two forms (kLean).  The default keeps the step of each
-// chain's maximum in shared memory (written at every raise, read only by the
-// rare re-decisions) to stay within 64 registers, and stages {RN64(d/R),
-// RN64(d*0.0174533)} per step.  The lean form, for lines of sight whose
-// tables would leave fewer than three CTAs per SM, holds the maximum's step in
-// registers, recomputes the surface addend from the staged f32 d (one DMUL,
-// the shape stage's own operation) and reads RN64(d/R) for the rare exact
-// re-decisions from the FP64 table in global memory.  Exact f32 holds its
-// running maximum exactly, in registers, and evaluates the reference's angle
-// wherever the first test passes.
+// MIXED64 comes in two forms (kLean).  Both keep the step of each chain's
+// maximum in registers, two 16-bit steps per register (TVS_MIX_JREG; written
+// at every raise, read only by the rare re-decisions).  The default stages
+// {RN64(d/R), RN64(d*0.0174533)} per step.  The lean form, for lines of sight
+// whose tables would leave fewer than three CTAs per SM, recomputes the
+// surface addend from the staged f32 d (one DMUL, the shape stage's own
+// operation) and reads RN64(d/R) for the rare exact re-decisions from the FP64
+// table in global memory.  Exact f32 holds its running maximum exactly, in
+// registers, and evaluates the reference's angle wherever the first test
+// passes.
 #ifndef TVS_EXACT_INLINE
 #define TVS_EXACT_INLINE 1
 #endif
@@ -126,6 +126,16 @@ template <> struct SplitTypes<TVS_PRECISION_FP32> {
 // instead of recomputing it.
 #ifndef TVS_MIX_RCP_TABLE
 #define TVS_MIX_RCP_TABLE 0
+#endif
+// MIXED64 keeps the step of each chain's maximum in registers, two 16-bit
+// steps per register (band tables of up to 65535 steps; 0 keeps it in shared
+// memory instead, 4 B per chain).
+#ifndef TVS_MIX_JREG
+#define TVS_MIX_JREG 1
+#endif
+
+#ifndef TVS_MIX_SELECT
+#define TVS_MIX_SELECT 0
 #endif
 
 // Shared-memory layout of one CTA.  Every array starts on 16 bytes.
@@ -150,7 +160,7 @@ template <int kPrec, bool kLean = false> struct SplitSmem {
         return fwd(cap) + (size_t)K * kQueueThreads * sizeof(S);
     }
     __host__ __device__ static size_t total(uint32_t cap) {
-        return jtab(cap) + (kPrec == TVS_PRECISION_MIXED64 && !kLean
+        return jtab(cap) + (kPrec == TVS_PRECISION_MIXED64 && !kLean && !TVS_MIX_JREG
                                 ? (size_t)K * kQueueThreads * sizeof(int32_t) : 0);
     }
 };
@@ -322,6 +332,12 @@ k_sweep_split(QueueArgs a) {
 #pragma unroll
             for (int k = 0; k < K; k++)
                 hp32[k] = __fadd_rn(__ldg(ep[k / KX] + LX * (k % KX)), D.observer_height);
+            // chain k's point-of-view elevation, re-read by the rare exact
+            // re-decisions (the address is recomputed rather than kept live)
+            auto pov_h = [&](int k) -> float {
+                const uint32_t r = min(ty + LY * (k / KX), D.row_end - 1);
+                return __ldg(D.elev + (int64_t)(r + D.los) * D.width + tx + LX * (k % KX) + D.los);
+            };
             uint32_t active = 0;  // chains on the grid (ring records)
 #pragma unroll
             for (int k = 0; k < K; k++)
@@ -554,19 +570,29 @@ k_sweep_split(QueueArgs a) {
                     for (int k = 0; k < K; k++) out[k] = sf[k];
                 } else {
                     // ---- guard band with exact re-decisions (MIXED64) ----------
-                    constexpr bool kJSmem = kMix && !kLean;
+                    constexpr bool kJSmem = kMix && !kLean && !TVS_MIX_JREG;
+                    constexpr bool kJPack = kMix && TVS_MIX_JREG;
                     float hi[K], lo[K];
                     // step of the running maximum (-1: the initial one)
                     int32_t jreg[kJSmem ? 1 : K] = {};
                     int32_t *sj = s_j + tid;
                     (void)jreg;
                     (void)sj;
+                    // packed: two chains' steps per register, 16 bits each
+                    // (0xffff: the initial maximum)
+                    uint32_t jpk[K / 2] = {};
+                    (void)jpk;
                     auto getj = [&](int k) -> int32_t {
                         if constexpr (kJSmem) return sj[k * kQueueThreads];
-                        else return jreg[k];
+                        else if constexpr (kJPack) {
+                            const uint32_t v = (jpk[k / 2] >> (16 * (k & 1))) & 0xffffu;
+                            return v == 0xffffu ? -1 : (int32_t)v;
+                        } else return jreg[k];
                     };
                     auto setj = [&](int k, int32_t v) {
                         if constexpr (kJSmem) sj[k * kQueueThreads] = v;
+                        else if constexpr (kJPack)
+                            jpk[k / 2] = __byte_perm(jpk[k / 2], (uint32_t)v, (k & 1) ? 0x5410 : 0x3254);
                         else jreg[k] = v;
                     };
                     S acc[K];
@@ -592,7 +618,7 @@ k_sweep_split(QueueArgs a) {
                     auto exact_at = [&](int k, uint32_t st, float h) -> S {
                         if constexpr (kMix) {
                             const double d = (double)s_t[st].w;
-                            const double hp64 = __dadd_rn((double)__ldg(ep[k / KX] + LX * (k % KX)),
+                            const double hp64 = __dadd_rn((double)pov_h(k),
                                                           (double)D.observer_height);
                             const double e = __dsub_rn((double)h, hp64);
 #if TVS_MIX_RCP_TABLE
@@ -648,16 +674,25 @@ k_sweep_split(QueueArgs a) {
                             else w = t.w;
 #pragma unroll
                             for (int k = 0; k < K; k++) {
-                                // surely visible: raise the window, without a branch
+                                const bool maybe = fh[k] >= lo[k];
+                                // surely visible: raise the window
                                 const float fl = __fmaf_rn(e[k], t.x, t.z);
                                 const bool sure = fl > hi[k];
-                                const bool maybe = fh[k] >= lo[k];
-                                hi[k] = sure ? __fmaf_rn(fabsf(fh[k]), kRel, fh[k]) : hi[k];
-                                lo[k] = sure ? __fmaf_rn(fabsf(fl), -kRel, fl) : lo[k];
-                                if (sure) setj(k, (int32_t)i);
-                                // adding +0 leaves a non-negative sum unchanged
-                                if constexpr (kMix) acc[k] = __dadd_rn(acc[k], sure ? w : 0.0);
-                                else acc[k] = __fadd_rn(acc[k], sure ? w : 0.0f);
+#if TVS_MIX_SELECT
+                                const float nhi = __fmaf_rn(fabsf(fh[k]), kRel, fh[k]);
+                                const float nlo = __fmaf_rn(fabsf(fl), -kRel, fl);
+                                hi[k] = sure ? nhi : hi[k];
+                                lo[k] = sure ? nlo : lo[k];
+#endif
+                                if (sure) {
+#if !TVS_MIX_SELECT
+                                    hi[k] = __fmaf_rn(fabsf(fh[k]), kRel, fh[k]);
+                                    lo[k] = __fmaf_rn(fabsf(fl), -kRel, fl);
+#endif
+                                    setj(k, (int32_t)i);
+                                    if constexpr (kMix) acc[k] = __dadd_rn(acc[k], w);
+                                    else acc[k] = __fadd_rn(acc[k], w);
+                                }
                                 vis |= (uint32_t)sure << k;
                                 amb |= (uint32_t)(!sure && maybe) << k;
                             }
@@ -691,7 +726,7 @@ k_sweep_split(QueueArgs a) {
                             S ang;
                             if constexpr (kMix) {
                                 const double d = (double)s_t[i].w;
-                                const double hp64 = __dadd_rn((double)__ldg(ep[k / KX] + LX * (k % KX)),
+                                const double hp64 = __dadd_rn((double)pov_h(k),
                                                               (double)D.observer_height);
                                 ang = __dsub_rn(__ddiv_rn(__dsub_rn((double)h, hp64), d), mix_c(i));
                             } else {
@@ -931,6 +966,7 @@ cudaError_t launch_sweep_split(const QueueArgs &a, int precision, int layout, cu
         return rings ? launch_split_layout<TVS_PRECISION_EXACT32, true>(a, layout, s)
                      : launch_split_layout<TVS_PRECISION_EXACT32, false>(a, layout, s);
     case TVS_PRECISION_MIXED64: {
+        if (TVS_MIX_JREG && a.max_step_cap > 0xffffu) return cudaErrorInvalidValue;  // 16-bit steps
         if (rings) return launch_split_layout<TVS_PRECISION_MIXED64, true>(a, layout, s);
         bool lean = false;
         const cudaError_t e = mix_lean(a.max_step_cap, &lean);
