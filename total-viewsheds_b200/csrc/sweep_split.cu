@@ -134,10 +134,6 @@ template <> struct SplitTypes<TVS_PRECISION_FP32> {
 #define TVS_MIX_JREG 1
 #endif
 
-#ifndef TVS_MIX_SELECT
-#define TVS_MIX_SELECT 0
-#endif
-
 // Shared-memory layout of one CTA.  Every array starts on 16 bytes.
 __host__ __device__ constexpr size_t align16(size_t n) { return (n + 15) & ~(size_t)15; }
 
@@ -312,10 +308,14 @@ k_sweep_split(QueueArgs a) {
             const uint32_t ty = D.row_begin + by * (kQueueTileY * LY * KY) + threadIdx.y * LY * KY + ly;
             // rows past the grid are clamped, columns past it read the padding
             // after the elevations; both are discarded (and record no rings)
-            const float *ep[KY];
+            auto row_ptr = [&](int r) -> const float * {
+                return D.elev + (int64_t)(min(ty + LY * r, D.row_end - 1) + D.los) * D.width + tx + D.los;
+            };
+            // the quad layout reads the plain DEM only on a few sectors: there
+            // the row pointers are recomputed instead of held in registers
+            const float *ep[kQuad ? 1 : KY];
 #pragma unroll
-            for (int r = 0; r < KY; r++)
-                ep[r] = D.elev + (int64_t)(min(ty + LY * r, D.row_end - 1) + D.los) * D.width + tx + D.los;
+            for (int r = 0; r < (kQuad ? 1 : KY); r++) ep[r] = row_ptr(r);
             // quad: the lane's base in the row-interleaved copies (rows past the
             // grid are not clamped: the copies hold zero rows for them)
             const char *qbase = nullptr;
@@ -331,7 +331,7 @@ k_sweep_split(QueueArgs a) {
             float hp32[K];  // kernel.rs:134, the f32 observer elevation
 #pragma unroll
             for (int k = 0; k < K; k++)
-                hp32[k] = __fadd_rn(__ldg(ep[k / KX] + LX * (k % KX)), D.observer_height);
+                hp32[k] = __fadd_rn(__ldg(row_ptr(k / KX) + LX * (k % KX)), D.observer_height);
             // chain k's point-of-view elevation, re-read by the rare exact
             // re-decisions (the address is recomputed rather than kept live)
             auto pov_h = [&](int k) -> float {
@@ -352,7 +352,8 @@ k_sweep_split(QueueArgs a) {
                 constexpr int dir = decltype(DIR)::value;
                 constexpr bool qplain = decltype(PLAIN)::value;
                 auto at = [&](long long b, int k) -> const float * {
-                    return (const float *)((const char *)ep[k / KX] + (dir ? -b : b)) + LX * (k % KX);
+                    const float *row = kQuad ? row_ptr(k / KX) : ep[k / KX];
+                    return (const float *)((const char *)row + (dir ? -b : b)) + LX * (k % KX);
                 };
                 // ring records of chain k: kernel id and the DEM id of a sample
                 // the four chains' samples at step st
@@ -678,17 +679,9 @@ k_sweep_split(QueueArgs a) {
                                 // surely visible: raise the window
                                 const float fl = __fmaf_rn(e[k], t.x, t.z);
                                 const bool sure = fl > hi[k];
-#if TVS_MIX_SELECT
-                                const float nhi = __fmaf_rn(fabsf(fh[k]), kRel, fh[k]);
-                                const float nlo = __fmaf_rn(fabsf(fl), -kRel, fl);
-                                hi[k] = sure ? nhi : hi[k];
-                                lo[k] = sure ? nlo : lo[k];
-#endif
                                 if (sure) {
-#if !TVS_MIX_SELECT
                                     hi[k] = __fmaf_rn(fabsf(fh[k]), kRel, fh[k]);
                                     lo[k] = __fmaf_rn(fabsf(fl), -kRel, fl);
-#endif
                                     setj(k, (int32_t)i);
                                     if constexpr (kMix) acc[k] = __dadd_rn(acc[k], w);
                                     else acc[k] = __fadd_rn(acc[k], w);
