@@ -535,6 +535,16 @@ int header_status(tvs_context *c, uint32_t first, uint32_t count) {
     return TVS_OK;
 }
 
+// The shape slot of one sector for the per-sector calls: computed (and its
+// status checked) once, then reused until a table is installed for it.
+int ensure_shape(tvs_context *c, uint32_t angle) {
+    if (c->shape_ok[angle]) return TVS_OK;
+    int rc = enqueue_shape(c, angle, 1);
+    if (rc == TVS_OK) rc = header_status(c, angle, 1);
+    if (rc == TVS_OK) c->shape_ok[angle] = true;
+    return rc;
+}
+
 // Copy one sector's ring records to the host and apply the spilled ids with
 // the reference's sequential semantics: band k writes slots k*R .. k*R+n_k
 // (kernel.rs:141-243), so an id past its own record lands in a later band's
@@ -885,9 +895,7 @@ int tvs_compute_sector(tvs_context *ctx, uint32_t angle, float *cumulative_surfa
                                       ctx->g.ring_slots_per_sector * sizeof(uint32_t), ctx->stream));
         TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), ctx->stream));
     }
-    int rc = enqueue_shape(ctx, angle, 1);
-    if (rc) return rc;
-    rc = header_status(ctx, angle, 1);
+    int rc = ensure_shape(ctx, angle);
     if (rc) return rc;
     rc = enqueue_sweep(ctx, angle, 1, rings ? R : 0);
     if (rc) return rc;
@@ -921,9 +929,7 @@ int tvs_compute_sector_rings(tvs_context *ctx, uint32_t angle, float *cumulative
         TVS_CUDA(ctx, cudaMalloc(&ctx->d_rc_blocks, (nb + 1) * sizeof(uint64_t)));
         ctx->device_bytes += (bands + 1 + nb + 1) * sizeof(uint64_t);
     }
-    int rc = enqueue_shape(ctx, angle, 1);
-    if (rc) return rc;
-    rc = header_status(ctx, angle, 1);
+    int rc = ensure_shape(ctx, angle);
     if (rc) return rc;
     // The sweep writes up to `slots` ids per band in place and the rest to the
     // spill list.  When a sector spills more than the list holds, the slots
@@ -952,8 +958,13 @@ int tvs_compute_sector_rings(tvs_context *ctx, uint32_t angle, float *cumulative
         TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), ctx->stream));
         rc = enqueue_sweep(ctx, angle, 1, R);
         if (rc) return rc;
+        // the record lengths (slot 0 holds a band's whole count, spilled ids
+        // included) are scanned before the spill check: one wait for both
+        TVS_CUDA(ctx, tvs::launch_ring_count(ctx->d_rings, bands, R, ctx->d_rc_blocks, ctx->stream));
         TVS_CUDA(ctx, cudaMemcpyAsync(cnt, ctx->d_counters, sizeof cnt, cudaMemcpyDeviceToHost,
                                       ctx->stream));
+        TVS_CUDA(ctx, cudaMemcpyAsync(&total, ctx->d_rc_blocks + nb, sizeof total,
+                                      cudaMemcpyDeviceToHost, ctx->stream));
         TVS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         if (cnt[0] <= ctx->spill_cap) break;
         if (R >= most)
@@ -963,10 +974,6 @@ int tvs_compute_sector_rings(tvs_context *ctx, uint32_t angle, float *cumulative
     if (count)
         TVS_CUDA(ctx, cudaMemcpyAsync(cumulative_surfaces, ctx->d_cum, count * sizeof(float),
                                       cudaMemcpyDeviceToHost, ctx->stream));
-    TVS_CUDA(ctx, tvs::launch_ring_count(ctx->d_rings, bands, R, ctx->d_rc_blocks, ctx->stream));
-    TVS_CUDA(ctx, cudaMemcpyAsync(&total, ctx->d_rc_blocks + nb, sizeof total,
-                                  cudaMemcpyDeviceToHost, ctx->stream));
-    TVS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (stats) {
         std::memset(stats, 0, sizeof *stats);
         stats->angle = angle;

@@ -96,15 +96,28 @@ k_ring_gather(const uint32_t *rings, uint64_t bands, uint32_t reserved, const ui
     }
     __shared__ uint64_t total;
     uint64_t off = block_base[blockIdx.x] + block_exclusive(s, &total);
+    uint64_t at[kRingPer];
 #pragma unroll
     for (int j = 0; j < kRingPer; j++) {
-        const uint64_t band = b0 + j;
-        if (band >= bands) break;
-        offsets[band] = off;
-        const uint32_t in_slots = min(len[j], reserved - 1);
-        const uint32_t *rec = rings + band * reserved + 1;
-        for (uint32_t q = 0; q < in_slots; q++) ids[off + q] = rec[q];
+        at[j] = off;
+        if (b0 + j < bands) offsets[b0 + j] = off;
         off += len[j];
+    }
+    // The warp copies its 32 x kRingPer records one at a time, in band order:
+    // lane q moves id q of the record, so each record is one coalesced read of
+    // its slots and one contiguous write.
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warp_b0 = (uint64_t)blockIdx.x * kRingChunk + (uint64_t)(threadIdx.x & ~31u) * kRingPer;
+    for (uint32_t src = 0; src < 32; src++) {
+#pragma unroll
+        for (int j = 0; j < kRingPer; j++) {
+            const uint64_t band = warp_b0 + (uint64_t)src * kRingPer + j;
+            const uint32_t n = __shfl_sync(0xffffffffu, min(len[j], reserved - 1), src);
+            const uint64_t o = __shfl_sync(0xffffffffu, at[j], src);
+            if (band >= bands) continue;  // uniform over the warp
+            const uint32_t *rec = rings + band * reserved + 1;
+            for (uint32_t q = lane; q < n; q += 32) ids[o + q] = rec[q];
+        }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) offsets[bands] = block_base[gridDim.x];
 }

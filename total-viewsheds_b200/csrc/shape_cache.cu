@@ -149,12 +149,14 @@ int tvs_set_band_shape(tvs_context *ctx, uint32_t angle, const int32_t *band_del
     TVS_CCUDA(ctx, cudaStreamSynchronize(ctx->stream));  // the host tables may go away
     if (!ctx->installed[angle]) tvs_host::drop_tvs_graph_of(ctx);  // one more shape launch
     ctx->installed[angle] = true;
+    ctx->shape_ok[angle] = false;
     return TVS_OK;
 }
 
 int tvs_clear_band_shapes(tvs_context *ctx) {
     if (!ctx) return TVS_ERR_INVALID_ARGUMENT;
     for (bool &b : ctx->installed) b = false;
+    for (bool &b : ctx->shape_ok) b = false;
     tvs_host::drop_tvs_graph_of(ctx);
     if (!ctx->d_installed) return TVS_OK;
     TVS_CCUDA(ctx, cudaSetDevice(ctx->p.device));

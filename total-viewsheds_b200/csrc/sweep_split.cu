@@ -169,9 +169,16 @@ template <int kPrec, bool kLean = false> struct SplitSmem {
 #ifndef TVS_SPLIT_BLOCKS32
 #define TVS_SPLIT_BLOCKS32 4
 #endif
+#ifndef TVS_SPLIT_RING_BLOCKS
+#define TVS_SPLIT_RING_BLOCKS 3
+#endif
+#ifndef TVS_SPLIT_RING_BLOCKS32
+#define TVS_SPLIT_RING_BLOCKS32 3
+#endif
 template <int kPrec, bool kRings>
 constexpr int split_min_blocks() {
-    return (kRings ? 3 : kPrec == TVS_PRECISION_MIXED64 ? TVS_SPLIT_MIX_BLOCKS : TVS_SPLIT_BLOCKS32) *
+    return (kPrec == TVS_PRECISION_MIXED64 ? (kRings ? TVS_SPLIT_RING_BLOCKS : TVS_SPLIT_MIX_BLOCKS)
+                                           : (kRings ? TVS_SPLIT_RING_BLOCKS32 : TVS_SPLIT_BLOCKS32)) *
            8 / kQueueTileY;
 }
 

@@ -62,6 +62,10 @@ struct tvs_context {
     float *d_tab_dists = nullptr;
     unsigned char *d_installed = nullptr;  // [180]
     bool installed[tvs::kSectorSteps] = {};
+    // sectors whose shape slot holds this context's shape with an OK status
+    // (the shape depends on the geometry and an installed table only, not on
+    // the elevations), so the per-sector calls skip the shape stage
+    bool shape_ok[tvs::kSectorSteps] = {};
     // compact ring records of the last tvs_compute_sector_rings (allocated on first use)
     uint64_t *d_rc_blocks = nullptr;   // scanned record-length block sums
     uint64_t *d_rc_offsets = nullptr;  // [total_bands + 1]
