@@ -527,26 +527,31 @@ def main():
         legs["exact32_engine"]["identical_to_plain_port"] = bool(np.array_equal(
             outs["exact32_engine"].view(np.uint32), outs["plain_port"].view(np.uint32)))
 
-    # Ring records of a whole TVS through the compact stream (one
-    # tvs_compute_sector_rings call per sector: the surfaces, the records of
-    # every band kept on the device); host-timed, every call synchronises.
+    # Ring records of a whole TVS through the compact stream: sectors in groups
+    # of RING_SECTORS per tvs_compute_sectors_rings call (one sweep launch per
+    # group; the surfaces and the records of every band kept on the device);
+    # host-timed, every call synchronises.
     rings_leg = None
     if not args.no_rings and args.kernel == "engine" and rows is None:
-        cum_r = np.zeros(eng.count, np.float32)
+        RING_SECTORS = 6
+        cum_r = torch.zeros(eng.count, dtype=torch.float32).pin_memory().numpy()
         total_ids = ctypes.c_uint64()
         st = tvs.SectorStats()
         L = tvs.lib()
-        L.tvs_compute_sector_rings(eng.ctx, 0, tvs._ptr(cum_r), ctypes.byref(total_ids),
-                                   ctypes.byref(st))  # allocates the record buffers
+
+        def ring_call(first):
+            rc = L.tvs_compute_sectors_rings(eng.ctx, first, RING_SECTORS, tvs._ptr(cum_r),
+                                             ctypes.byref(total_ids), ctypes.byref(st))
+            if rc:
+                raise tvs.TvsError(rc, L.tvs_last_error(eng.ctx).decode())
+
+        ring_call(0)  # allocates the record buffers
         cum_r[:] = 0
         ids_all, most = 0, 0
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
-        for a in range(SECTORS):
-            rc = L.tvs_compute_sector_rings(eng.ctx, a, tvs._ptr(cum_r), ctypes.byref(total_ids),
-                                            ctypes.byref(st))
-            if rc:
-                raise tvs.TvsError(rc, L.tvs_last_error(eng.ctx).decode())
+        for first in range(0, SECTORS, RING_SECTORS):
+            ring_call(first)
             ids_all += total_ids.value
             most = max(most, st.max_ring_ids)
         t_rings = time.perf_counter() - t0
@@ -554,9 +559,10 @@ def main():
                      "record_bytes_per_tvs": 4 * ids_all + 8 * (g.total_bands + 1) * SECTORS,
                      "most_ids_in_a_band": most,
                      "vs_surfaces_only": t_rings / (total_ms / args.steps * 1e-3),
-                     "path": "tvs_compute_sector_rings per sector: H2D + D2H of the surfaces, "
-                             "shape stage, split sweep writing ring slots, scan + gather into "
-                             "the compact stream (host-timed)"}
+                     "sectors_per_call": RING_SECTORS,
+                     "path": f"tvs_compute_sectors_rings, {RING_SECTORS} sectors per call: H2D + D2H "
+                             "of the surfaces (pinned), one split-sweep launch writing ring slots, "
+                             "scan + gather into the compact stream (host-timed)"}
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define TVS_ABI_VERSION 4
+#define TVS_ABI_VERSION 5
 
 /* Status codes.  Negative values are errors; tvs_last_error() has the text. */
 enum tvs_status {
@@ -203,6 +203,22 @@ int tvs_compute_sector(tvs_context *ctx, uint32_t angle, float *cumulative_surfa
  * No counterpart in the reference; the records equal its per-band records. */
 int tvs_compute_sector_rings(tvs_context *ctx, uint32_t angle, float *cumulative_surfaces,
                              uint64_t *total_ids, tvs_sector_stats *stats);
+/* Sectors [first_angle, first_angle + n_sectors) in one sweep launch, as
+ * Compute::run's loop takes them (compute.rs:106-112): cumulative_surfaces
+ * advances by every sector in order (FP64 and MIXED64 keep double between the
+ * call's sectors, as tvs_run does), and the records of all of them form one
+ * compact stream in which sector first_angle + s owns records
+ * s * total_bands .. (s + 1) * total_bands - 1.  stats aggregates the sectors
+ * (angle = first_angle).  More than one sector needs the persistent split
+ * sweep (not FP64 or the plain kernel); the slots behind the stream take
+ * n_sectors * total_bands * 64 u32 of device memory.  No counterpart in the
+ * reference (it computes one sector per call). */
+int tvs_compute_sectors_rings(tvs_context *ctx, uint32_t first_angle, uint32_t n_sectors,
+                              float *cumulative_surfaces, uint64_t *total_ids,
+                              tvs_sector_stats *stats);
+/* The records of the last tvs_compute_sector_rings or tvs_compute_sectors_rings
+ * call: band_offsets [records + 1] (records = n_sectors * total_bands) and
+ * ids [*total_ids], either nullable. */
 int tvs_read_ring_records(tvs_context *ctx, uint64_t *band_offsets, uint32_t *ids);
 
 /* Compute::run (compute.rs:101-115): all 180 sectors.  cumulative_out and

@@ -25,7 +25,7 @@ def test_library_exports_every_declared_symbol(tvs):
     lib = tvs.lib()
     for name in header_functions():
         assert hasattr(lib, name), name
-    assert lib.tvs_abi_version() == 4
+    assert lib.tvs_abi_version() == 5
 
 
 def test_struct_layouts(tvs):

@@ -120,6 +120,7 @@ SIGNATURES = {
     "tvs_band_shape": (_INT, [_VP, _U32, _VP, _VP, _P(_U32)]),
     "tvs_set_band_shape": (_INT, [_VP, _U32, _VP, _VP, _U64]),
     "tvs_compute_sector_rings": (_INT, [_VP, _U32, _VP, _P(_U64), _P(SectorStats)]),
+    "tvs_compute_sectors_rings": (_INT, [_VP, _U32, _U32, _VP, _P(_U64), _P(SectorStats)]),
     "tvs_read_ring_records": (_INT, [_VP, _VP, _VP]),
     "tvs_clear_band_shapes": (_INT, [_VP]),
     "tvs_cache_load": (_INT, [_VP, ctypes.c_char_p, _P(_U32)]),
@@ -290,6 +291,21 @@ class Engine:
         self._check(lib().tvs_compute_sector_rings(self.ctx, angle, _ptr(cumulative),
                                                    ctypes.byref(total), ctypes.byref(st)))
         offsets = np.empty(self.geometry.total_bands + 1, np.uint64)
+        ids = np.empty(max(total.value, 1), np.uint32)
+        self._check(lib().tvs_read_ring_records(self.ctx, _ptr(offsets), _ptr(ids)))
+        return offsets, ids[:total.value], st
+
+    def compute_sectors_rings(self, first_angle, n_sectors, cumulative):
+        """Sectors first_angle .. first_angle + n_sectors - 1 in one launch, in
+        place on cumulative: (band_offsets u64 [n_sectors * total_bands + 1], ids
+        u32, SectorStats); band k of sector first_angle + s is record
+        s * total_bands + k."""
+        assert cumulative.dtype == np.float32 and cumulative.flags.c_contiguous
+        total = ctypes.c_uint64()
+        st = SectorStats()
+        self._check(lib().tvs_compute_sectors_rings(self.ctx, first_angle, n_sectors, _ptr(cumulative),
+                                                    ctypes.byref(total), ctypes.byref(st)))
+        offsets = np.empty(n_sectors * self.geometry.total_bands + 1, np.uint64)
         ids = np.empty(max(total.value, 1), np.uint32)
         self._check(lib().tvs_read_ring_records(self.ctx, _ptr(offsets), _ptr(ids)))
         return offsets, ids[:total.value], st

@@ -915,32 +915,54 @@ int tvs_compute_sector(tvs_context *ctx, uint32_t angle, float *cumulative_surfa
     return TVS_OK;
 }
 
-int tvs_compute_sector_rings(tvs_context *ctx, uint32_t angle, float *cumulative_surfaces,
-                             uint64_t *total_ids, tvs_sector_stats *stats) {
+int tvs_compute_sectors_rings(tvs_context *ctx, uint32_t first_angle, uint32_t n_sectors,
+                              float *cumulative_surfaces, uint64_t *total_ids,
+                              tvs_sector_stats *stats) {
     if (!ctx || !cumulative_surfaces || !total_ids) return TVS_ERR_INVALID_ARGUMENT;
-    if (angle >= tvs::kSectorSteps) return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "angle >= 180");
+    if (n_sectors == 0 || first_angle >= tvs::kSectorSteps ||
+        n_sectors > tvs::kSectorSteps - first_angle)
+        return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "sectors outside 0..179 (or none)");
+    // several sectors in one launch: the direction-split sweep only
+    if (n_sectors > 1 && (ctx->p.precision == TVS_PRECISION_FP64 ||
+                          ctx->p.sweep_kernel == TVS_SWEEP_PLAIN || sweep_impl() != SweepImpl::Queue))
+        return fail(ctx, TVS_ERR_INVALID_ARGUMENT,
+                    "ring records of several sectors per call need the persistent split sweep "
+                    "(not FP64 or the plain kernel)");
     TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
     ctx->rc_valid = false;
     const uint64_t count = ctx->g.computable_points_count;
-    const uint64_t bands = ctx->g.total_bands;
-    const uint64_t nb = tvs::ring_scan_blocks(bands);
-    if (!ctx->d_rc_offsets) {
-        TVS_CUDA(ctx, cudaMalloc(&ctx->d_rc_offsets, (bands + 1) * sizeof(uint64_t)));
+    const uint64_t recs = ctx->g.total_bands * n_sectors;  // records of this call
+    const uint64_t nb = tvs::ring_scan_blocks(recs);
+    if (!ctx->d_rc_offsets || recs > ctx->rc_records_cap) {
+        if (ctx->d_rc_offsets) {
+            cudaFree(ctx->d_rc_offsets);
+            cudaFree(ctx->d_rc_blocks);
+            ctx->device_bytes -= (ctx->rc_records_cap + 1 + tvs::ring_scan_blocks(ctx->rc_records_cap) + 1) *
+                                 sizeof(uint64_t);
+            ctx->d_rc_offsets = nullptr;
+            ctx->d_rc_blocks = nullptr;
+            ctx->rc_records_cap = 0;
+        }
+        TVS_CUDA(ctx, cudaMalloc(&ctx->d_rc_offsets, (recs + 1) * sizeof(uint64_t)));
         TVS_CUDA(ctx, cudaMalloc(&ctx->d_rc_blocks, (nb + 1) * sizeof(uint64_t)));
-        ctx->device_bytes += (bands + 1 + nb + 1) * sizeof(uint64_t);
+        ctx->rc_records_cap = recs;
+        ctx->device_bytes += (recs + 1 + nb + 1) * sizeof(uint64_t);
     }
-    int rc = ensure_shape(ctx, angle);
-    if (rc) return rc;
+    for (uint32_t a = first_angle; a < first_angle + n_sectors; a++) {
+        int rc = ensure_shape(ctx, a);
+        if (rc) return rc;
+    }
     // The sweep writes up to `slots` ids per band in place and the rest to the
-    // spill list.  When a sector spills more than the list holds, the slots
-    // per band double and the sector runs again from the caller's surfaces (a
+    // spill list.  When the sectors spill more than the list holds, the slots
+    // per band double and the call runs again from the caller's surfaces (a
     // band has at most n_steps + 2 ids, so this ends).
     const uint32_t most = ctx->g.band_steps_filled + 4;
     uint32_t R = 0, cnt[4];
     uint64_t total = 0;
+    int rc = TVS_OK;
     for (;;) {
         R = std::min(ctx->compact_slots, most);
-        rc = ensure_rings(ctx, R);
+        rc = ensure_rings(ctx, R * n_sectors);  // [sector][band][R]
         if (rc) return rc;
         if (count)
             TVS_CUDA(ctx, cudaMemcpyAsync(ctx->d_cum, cumulative_surfaces, count * sizeof(float),
@@ -954,13 +976,13 @@ int tvs_compute_sector_rings(tvs_context *ctx, uint32_t angle, float *cumulative
         if (ctx->row_begin != 0 || ctx->row_end != ctx->g.tvs_height ||
             ctx->p.sweep_kernel == TVS_SWEEP_PLAIN || ctx->p.precision == TVS_PRECISION_FP64 ||
             sweep_impl() != SweepImpl::Queue)
-            TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_rings, 0, bands * R * sizeof(uint32_t), ctx->stream));
+            TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_rings, 0, recs * R * sizeof(uint32_t), ctx->stream));
         TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), ctx->stream));
-        rc = enqueue_sweep(ctx, angle, 1, R);
+        rc = enqueue_sweep(ctx, first_angle, n_sectors, R);
         if (rc) return rc;
         // the record lengths (slot 0 holds a band's whole count, spilled ids
         // included) are scanned before the spill check: one wait for both
-        TVS_CUDA(ctx, tvs::launch_ring_count(ctx->d_rings, bands, R, ctx->d_rc_blocks, ctx->stream));
+        TVS_CUDA(ctx, tvs::launch_ring_count(ctx->d_rings, recs, R, ctx->d_rc_blocks, ctx->stream));
         TVS_CUDA(ctx, cudaMemcpyAsync(cnt, ctx->d_counters, sizeof cnt, cudaMemcpyDeviceToHost,
                                       ctx->stream));
         TVS_CUDA(ctx, cudaMemcpyAsync(&total, ctx->d_rc_blocks + nb, sizeof total,
@@ -976,7 +998,7 @@ int tvs_compute_sector_rings(tvs_context *ctx, uint32_t angle, float *cumulative
                                       cudaMemcpyDeviceToHost, ctx->stream));
     if (stats) {
         std::memset(stats, 0, sizeof *stats);
-        stats->angle = angle;
+        stats->angle = first_angle;
         stats->band_steps_filled = ctx->g.band_steps_filled;
         stats->overflow_bands = cnt[1];
         stats->max_ring_ids = cnt[2];
@@ -989,21 +1011,28 @@ int tvs_compute_sector_rings(tvs_context *ctx, uint32_t angle, float *cumulative
             ctx->d_rc_ids = nullptr;
             ctx->rc_ids_cap = 0;
         }
-        const uint64_t cap = total + total / 4;  // room for the next sectors
+        const uint64_t cap = total + total / 4;  // room for the next calls
         TVS_CUDA(ctx, cudaMalloc(&ctx->d_rc_ids, std::max<uint64_t>(cap, 1) * sizeof(uint32_t)));
         ctx->rc_ids_cap = std::max<uint64_t>(cap, 1);
         ctx->device_bytes += ctx->rc_ids_cap * sizeof(uint32_t);
     }
-    if (bands == 0)
+    if (recs == 0)
         TVS_CUDA(ctx, cudaMemsetAsync(ctx->d_rc_offsets, 0, sizeof(uint64_t), ctx->stream));
-    TVS_CUDA(ctx, tvs::launch_ring_gather(ctx->d_rings, bands, R, ctx->d_rc_blocks, ctx->d_spill,
+    TVS_CUDA(ctx, tvs::launch_ring_gather(ctx->d_rings, recs, R, ctx->d_rc_blocks, ctx->d_spill,
                                           cnt[0], ctx->d_rc_offsets, ctx->d_rc_ids, ctx->stream));
     ctx->launches += 2;
     TVS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     ctx->rc_total = total;
+    ctx->rc_records = recs;
     ctx->rc_valid = true;
     *total_ids = total;
     return TVS_OK;
+}
+
+int tvs_compute_sector_rings(tvs_context *ctx, uint32_t angle, float *cumulative_surfaces,
+                             uint64_t *total_ids, tvs_sector_stats *stats) {
+    if (ctx && angle >= tvs::kSectorSteps) return fail(ctx, TVS_ERR_INVALID_ARGUMENT, "angle >= 180");
+    return tvs_compute_sectors_rings(ctx, angle, 1, cumulative_surfaces, total_ids, stats);
 }
 
 int tvs_read_ring_records(tvs_context *ctx, uint64_t *band_offsets, uint32_t *ids) {
@@ -1013,7 +1042,7 @@ int tvs_read_ring_records(tvs_context *ctx, uint64_t *band_offsets, uint32_t *id
     TVS_CUDA(ctx, cudaSetDevice(ctx->p.device));
     if (band_offsets)
         TVS_CUDA(ctx, cudaMemcpyAsync(band_offsets, ctx->d_rc_offsets,
-                                      (ctx->g.total_bands + 1) * sizeof(uint64_t),
+                                      (ctx->rc_records + 1) * sizeof(uint64_t),
                                       cudaMemcpyDeviceToHost, ctx->stream));
     if (ids && ctx->rc_total)
         TVS_CUDA(ctx, cudaMemcpyAsync(ids, ctx->d_rc_ids, ctx->rc_total * sizeof(uint32_t),

@@ -393,9 +393,11 @@ k_sweep_split(QueueArgs a) {
                     else
                         return s_boff[st];
                 };
+                // a launch over several sectors keeps each sector's records
+                // apart: sector s of the launch owns records s * total_bands ..
                 auto kid = [&](int k) -> uint64_t {
                     return (uint64_t)(ty + LY * (k / KX)) * D.tvs_width + tx + LX * (k % KX) +
-                           (dir ? a.half_bands : 0);
+                           (dir ? a.half_bands : 0) + (uint64_t)s * 2 * a.half_bands;
                 };
                 auto dem_id = [&](int k, long long b) -> uint32_t {
                     const long long pov = (long long)(ty + LY * (k / KX) + D.los) * D.width +
@@ -959,7 +961,7 @@ size_t split_smem_bytes(int precision, uint32_t step_cap) {
 cudaError_t launch_sweep_split(const QueueArgs &a, int precision, int layout, cudaStream_t s) {
     if (a.n_dems == 0 || a.tiles_per_sector == 0 || a.n_sectors == 0) return cudaSuccess;
     const bool rings = a.rings != nullptr;
-    if (rings && (a.n_sectors != 1 || !a.ring_counters || !a.spill || a.ring_reserved < 2))
+    if (rings && (!a.ring_counters || !a.spill || a.ring_reserved < 2))
         return cudaErrorInvalidValue;
     switch (precision) {
     case TVS_PRECISION_EXACT32:

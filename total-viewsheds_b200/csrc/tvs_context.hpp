@@ -71,6 +71,8 @@ struct tvs_context {
     uint64_t *d_rc_offsets = nullptr;  // [total_bands + 1]
     uint32_t *d_rc_ids = nullptr;
     uint64_t rc_ids_cap = 0, rc_total = 0;
+    uint64_t rc_records = 0;      // records of the last call (sectors x total_bands)
+    uint64_t rc_records_cap = 0;  // records d_rc_offsets and d_rc_blocks hold
     bool rc_valid = false;
     // sweep counters (tvs_set_sweep_counters): [0] warp-steps swept, [1] past
     // the first test, [2] in all, [3] spare
