@@ -535,15 +535,30 @@ int header_status(tvs_context *c, uint32_t first, uint32_t count) {
     return TVS_OK;
 }
 
-// The shape slot of one sector for the per-sector calls: computed (and its
-// status checked) once, then reused until a table is installed for it.
-int ensure_shape(tvs_context *c, uint32_t angle) {
-    if (c->shape_ok[angle]) return TVS_OK;
-    int rc = enqueue_shape(c, angle, 1);
-    if (rc == TVS_OK) rc = header_status(c, angle, 1);
-    if (rc == TVS_OK) c->shape_ok[angle] = true;
-    return rc;
+// The shape slots of sectors [first, first+count) for the per-sector calls:
+// computed (one launch per run of missing sectors, one status check) once,
+// then reused until a table is installed for the sector.
+int ensure_shapes(tvs_context *c, uint32_t first, uint32_t count) {
+    bool launched = false;
+    for (uint32_t s = first; s < first + count;) {
+        if (c->shape_ok[s]) {
+            s++;
+            continue;
+        }
+        uint32_t e = s;
+        while (e < first + count && !c->shape_ok[e]) e++;
+        int rc = enqueue_shape(c, s, e - s);
+        if (rc) return rc;
+        launched = true;
+        s = e;
+    }
+    if (!launched) return TVS_OK;
+    int rc = header_status(c, first, count);
+    if (rc) return rc;
+    for (uint32_t s = first; s < first + count; s++) c->shape_ok[s] = true;
+    return TVS_OK;
 }
+int ensure_shape(tvs_context *c, uint32_t angle) { return ensure_shapes(c, angle, 1); }
 
 // Copy one sector's ring records to the host and apply the spilled ids with
 // the reference's sequential semantics: band k writes slots k*R .. k*R+n_k
@@ -948,8 +963,8 @@ int tvs_compute_sectors_rings(tvs_context *ctx, uint32_t first_angle, uint32_t n
         ctx->rc_records_cap = recs;
         ctx->device_bytes += (recs + 1 + nb + 1) * sizeof(uint64_t);
     }
-    for (uint32_t a = first_angle; a < first_angle + n_sectors; a++) {
-        int rc = ensure_shape(ctx, a);
+    {
+        int rc = ensure_shapes(ctx, first_angle, n_sectors);
         if (rc) return rc;
     }
     // The sweep writes up to `slots` ids per band in place and the rest to the
