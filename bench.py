@@ -302,6 +302,26 @@ def traffic_from_profiles(kernel_name):
         return None
 
 
+def targets(value, legs, precision):
+    """Which engine meets which half of the target: the reference CPU ring
+    records bit for bit, per-point surface error <= 1e-5 against FP64, and the
+    headline against the plain FP32 GPU sweeps."""
+    exact = legs["exact32_engine"]["surfaces_vs_fp64"]
+    return {
+        "reference_cpu_ring_records_bit_for_bit":
+            "exact32 engine (its surfaces equal the plain port's: "
+            f"{legs['exact32_engine'].get('identical_to_plain_port')}); MIXED64 records are the "
+            "FP64 ones, which differ from the reference's f32 records at ties",
+        "surface_rel_error_le_1e-5_vs_fp64": {
+            "headline": precision in ("mixed64", "fp64"),
+            "fp32_form": legs["plain_fp32_sweep"]["surfaces_vs_fp64"]["rel_max"] <= 1e-5
+            if legs["plain_fp32_sweep"]["surfaces_vs_fp64"] else None,
+            "exact32": exact["rel_max"] <= 1e-5 if exact else None},
+        "headline_over_plain_port": value / legs["plain_port"]["value"],
+        "headline_over_fp32_form": value / legs["plain_fp32_sweep"]["value"],
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -640,6 +660,7 @@ def main():
             **({"row_split": gathered} if gathered else {}),
             **({"rings_compact": rings_leg} if rings_leg else {}),
             **legs,
+            **({"targets": targets(value, legs, args.precision)} if legs else {}),
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

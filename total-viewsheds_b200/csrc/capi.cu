@@ -1026,7 +1026,9 @@ int tvs_compute_sectors_rings(tvs_context *ctx, uint32_t first_angle, uint32_t n
             ctx->d_rc_ids = nullptr;
             ctx->rc_ids_cap = 0;
         }
-        const uint64_t cap = total + total / 4;  // room for the next calls
+        // twice the need: sectors' record counts vary, and a reallocation
+        // (free + malloc of gigabytes) costs more than the spare memory
+        const uint64_t cap = 2 * total;
         TVS_CUDA(ctx, cudaMalloc(&ctx->d_rc_ids, std::max<uint64_t>(cap, 1) * sizeof(uint32_t)));
         ctx->rc_ids_cap = std::max<uint64_t>(cap, 1);
         ctx->device_bytes += ctx->rc_ids_cap * sizeof(uint32_t);
