@@ -2,7 +2,7 @@
 
 The 3601^2 precision form (ridged multifractal with a flat 0 m sea, 1200-cell
 line of sight) at the sectors where the reference's cost and tie behaviour
-differ most (0, 1, 45, 46 and 90 degrees: README.md:110 notes that 0 degrees
+differ most (0, 1, 45, 46 and 90 degrees: the reference's README.md:110 notes that 0 degrees
 is far faster than 1), the 7201^2 large region, and the 48-tile batching set.
 Integer data (ring records) and the exact-f32 surfaces must match the oracle
 bit for bit; MIXED64 and FP64 must match the oracle's all-FP64 restatement bit
