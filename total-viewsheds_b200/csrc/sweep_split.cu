@@ -968,7 +968,9 @@ cudaError_t launch_sweep_split(const QueueArgs &a, int precision, int layout, cu
         return rings ? launch_split_layout<TVS_PRECISION_EXACT32, true>(a, layout, s)
                      : launch_split_layout<TVS_PRECISION_EXACT32, false>(a, layout, s);
     case TVS_PRECISION_MIXED64: {
-        if (TVS_MIX_JREG && a.max_step_cap > 0xffffu) return cudaErrorInvalidValue;  // 16-bit steps
+        // 16-bit steps (0xffff marks the initial maximum): at most 65535 steps,
+        // a step table of at most 65536 entries (its length rounds up to 4)
+        if (TVS_MIX_JREG && a.max_step_cap > 0x10000u) return cudaErrorInvalidValue;
         if (rings) return launch_split_layout<TVS_PRECISION_MIXED64, true>(a, layout, s);
         bool lean = false;
         const cudaError_t e = mix_lean(a.max_step_cap, &lean);
